@@ -1,0 +1,158 @@
+"""ctypes binding of ``libdoe_b200.so`` (the C ABI declared in include/doe_b200.h).
+
+The engine has no CPU implementation: importing the package is cheap, but the
+first call that needs the device raises :class:`EngineUnavailable` when the
+library is missing or no CUDA device is visible. Nothing here falls back to host
+arithmetic.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdoe_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "doe_b200.h")
+
+DOE_OK = 0
+DOE_ERR_NOT_POW2 = 1
+DOE_ERR_SIZE_MISMATCH = 2
+DOE_ERR_BAD_ARG = 3
+DOE_ERR_CUDA = 4
+DOE_ERR_TIMEOUT = 5
+DOE_ERR_UNSUPPORTED = 6
+DOE_ERR_NO_DEVICE = 7
+
+
+class DOEError(Exception):
+    """Raised for a non-zero doe_status; ``code`` holds the status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class EngineUnavailable(RuntimeError):
+    """The CUDA engine cannot run here (library not built or no GPU)."""
+
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+_lib = None
+_lock = threading.Lock()
+
+
+def _declare(L):
+    i, d, u64 = C.c_int, C.c_double, C.c_ulonglong
+    ctxp = C.c_void_p
+    sig = {
+        "doe_abi_version": (i, []),
+        "doe_ctx_create": (i, [i, C.POINTER(C.c_void_p)]),
+        "doe_ctx_destroy": (None, [ctxp]),
+        "doe_last_error": (C.c_char_p, [ctxp]),
+        "doe_ctx_stream": (C.c_void_p, [ctxp]),
+        "doe_ctx_synchronize": (i, [ctxp]),
+        "doe_host_alloc": (i, [ctxp, C.POINTER(C.c_void_p), u64]),
+        "doe_host_free": (i, [ctxp, _vp]),
+        "doe_fft2d": (i, [ctxp, _dp, _dp, i, i, i]),
+        "doe_asm_transfer": (i, [ctxp, i, i, d, d, d, d, i, i, d, _dp, _dp, _dp]),
+        "doe_asm": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, i, i, d]),
+        "doe_asm_sweep": (i, [ctxp, _dp, _dp, i, i, d, d, d, _dp, i, i, i, d, _dp, _dp]),
+        "doe_focal_plane": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, _dp, _dp, _dp]),
+        "doe_fft2d_dev": (i, [ctxp, _vp, i, i, i, i]),
+        "doe_asm_sweep_dev": (i, [ctxp, _vp, i, i, i, d, d, _dp, _dp, i, i, i, d, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+def load_library():
+    """Load (not build) the engine library; raise EngineUnavailable if absent."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise EngineUnavailable(
+                    f"{LIB_PATH} is missing: build it with "
+                    "`python -m diffractiveopticalelement_b200.build` (needs nvcc)")
+            _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def declared_functions() -> list[str]:
+    """Entry points declared in include/doe_b200.h."""
+    import re
+    src = open(HEADER).read()
+    return re.findall(r"^\s*(?:int|void|const char\s*\*|void\s*\*)\s*(doe_\w+)\s*\(", src, re.M)
+
+
+class Context:
+    """One engine context (CUDA stream + scratch) on one device."""
+
+    def __init__(self, device: int = 0):
+        L = load_library()
+        h = C.c_void_p()
+        rc = L.doe_ctx_create(int(device), C.byref(h))
+        if rc == DOE_ERR_NO_DEVICE:
+            raise EngineUnavailable("no CUDA device is visible: the engine has no CPU path")
+        if rc != DOE_OK:
+            raise DOEError(rc, f"doe_ctx_create failed with status {rc}")
+        self.h = h
+        self.device = device
+        self.lib = L
+
+    def check(self, rc: int):
+        if rc != DOE_OK:
+            msg = self.lib.doe_last_error(self.h)
+            msg = msg.decode() if msg else f"status {rc}"
+            raise DOEError(rc, msg)
+
+    def synchronize(self):
+        self.check(self.lib.doe_ctx_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.doe_ctx_stream(self.h) or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.doe_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx: dict[int, Context] = {}
+
+
+def context(device: int | None = None) -> Context:
+    """Shared per-thread-agnostic default context for `device` (default 0)."""
+    dev = 0 if device is None else int(device)
+    with _lock:
+        c = _ctx.get(dev)
+    if c is None:
+        c = Context(dev)
+        with _lock:
+            _ctx[dev] = c
+    return c
+
+
+def f64(a) -> np.ndarray:
+    """C-contiguous float64 view/copy of a plane."""
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def dp(a):
+    return None if a is None else a.ctypes.data_as(_dp)

@@ -1,0 +1,332 @@
+// fft_core.cuh -- shared-memory Stockham FFT for sm_100a with fusable operators.
+//
+// One CTA transforms V independent vectors of compile-time power-of-two length N.
+// Each vector is handled by T = N / RMAX threads that keep RMAX complex values in
+// registers; passes exchange data through shared memory (Stockham autosort, so
+// no bit reversal is ever materialised). The first pass reads straight from
+// global memory through a caller-supplied load operator and the last pass hands
+// its values to a store operator, so pointwise work (shifts, transfer functions,
+// amplitude constraints, reductions, FP64<->FP32 conversion) is fused into the
+// transform instead of costing extra HBM round trips.
+//
+// Numerical contract: FP32 arithmetic with twiddles rounded once from FP64
+// (table `tw`, e^{-2 pi i m/N}), inner radix constants evaluated at compile time
+// from a Taylor series in double precision. Forward transform is unscaled and the
+// inverse carries no scale here; callers fold 1/(nx*ny) into a store, matching
+// the reference's fft2d (src/fft.js:148-154) up to FP32 rounding.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace doe {
+
+// ---------------------------------------------------------------- complex helpers
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// ---------------------------------------------------------------- compile-time trig
+// Maclaurin series for sin/cos on |x| <= pi/4 in double precision; only ever
+// evaluated by the compiler to produce the inner radix constants.
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double ct_sin_small(double x) {
+  double x2 = x * x, term = x, sum = x;
+  for (int i = 1; i < 14; ++i) {
+    term *= -x2 / double((2 * i) * (2 * i + 1));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double ct_cos_small(double x) {
+  double x2 = x * x, term = 1.0, sum = 1.0;
+  for (int i = 1; i < 14; ++i) {
+    term *= -x2 / double((2 * i - 1) * (2 * i));
+    sum += term;
+  }
+  return sum;
+}
+// cos(2 pi k / L) and sin(2 pi k / L) for integers, by octant symmetry.
+constexpr double ct_cos2pi(long k, long L) {
+  k %= L;
+  if (k < 0) k += L;
+  // reduce to [0, L/2]: cos is even around L/2 mirror
+  if (2 * k > L) k = L - k;                     // cos(2pi - a) = cos a
+  if (4 * k > L) return -ct_cos2pi(L / 2 - k, L);  // cos(pi - a) = -cos a  (k in (L/4, L/2])
+  // now a = 2 pi k / L in [0, pi/2]
+  if (8 * k > L) return ct_sin_small(2.0 * kPi * double(L / 4 - k) / double(L)) ;
+  return ct_cos_small(2.0 * kPi * double(k) / double(L));
+}
+constexpr double ct_sin2pi(long k, long L) { return ct_cos2pi(k - L / 4, L); }  // sin a = cos(a - pi/2)
+
+// ---------------------------------------------------------------- twiddled multiply
+// v * W_L^k with W_L = e^{-2 pi i / L} (forward) or its conjugate (inverse).
+// Exact special cases avoid multiplications by 0/1 that IEEE rules keep alive.
+template <int K, int L, bool INV>
+__device__ __forceinline__ float2 twiddle_const(float2 v) {
+  constexpr int k = ((K % L) + L) % L;
+  if constexpr (k == 0) {
+    return v;
+  } else if constexpr (2 * k == L) {
+    return make_float2(-v.x, -v.y);
+  } else if constexpr (4 * k == L) {  // -i (fwd) / +i (inv)
+    return INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  } else if constexpr (4 * k == 3 * L) {  // +i (fwd) / -i (inv)
+    return INV ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  } else {
+    constexpr float c = (float)ct_cos2pi(k, L);
+    constexpr float s = (float)(INV ? ct_sin2pi(k, L) : -ct_sin2pi(k, L));
+    if constexpr (8 * k == L || 8 * k == 3 * L || 8 * k == 5 * L || 8 * k == 7 * L) {
+      // |c| == |s| == sqrt(1/2): 2 multiplies instead of 4
+      constexpr float a = c;
+      constexpr float b = s;
+      if constexpr ((a > 0) == (b > 0)) {  // (a, a)
+        return make_float2(a * (v.x - v.y), a * (v.x + v.y));
+      } else {  // (a, -a)
+        return make_float2(a * (v.x + v.y), a * (v.y - v.x));
+      }
+    } else {
+      return make_float2(fmaf(v.x, c, -v.y * s), fmaf(v.x, s, v.y * c));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- register DFT
+// In-register radix-2 decimation-in-frequency DFT of R points stored in v[OFF..OFF+R),
+// natural order in and out (the bit reversal is a compile-time register rename).
+template <int R>
+struct Log2 {
+  static constexpr int value = (R <= 1) ? 0 : 1 + Log2<R / 2>::value;
+};
+template <>
+struct Log2<1> {
+  static constexpr int value = 0;
+};
+
+template <int R>
+__device__ __forceinline__ constexpr int bitrev(int i) {
+  int r = 0;
+  for (int b = 0; b < Log2<R>::value; ++b)
+    if (i & (1 << b)) r |= 1 << (Log2<R>::value - 1 - b);
+  return r;
+}
+
+template <int L, int HALF, int K, bool INV, int NBLK, int B, int OFF, int RA>
+struct DifStage {
+  // butterfly k of block b within a stage whose sub-length is L
+  static __device__ __forceinline__ void run(float2 (&v)[RA]) {
+    constexpr int i0 = OFF + B * L + K;
+    constexpr int i1 = i0 + HALF;
+    float2 a = v[i0], c = v[i1];
+    v[i0] = cadd(a, c);
+    v[i1] = twiddle_const<K, L, INV>(csub(a, c));
+    if constexpr (K + 1 < HALF) {
+      DifStage<L, HALF, K + 1, INV, NBLK, B, OFF, RA>::run(v);
+    } else if constexpr (B + 1 < NBLK) {
+      DifStage<L, HALF, 0, INV, NBLK, B + 1, OFF, RA>::run(v);
+    }
+  }
+};
+
+template <int R, int L, bool INV, int OFF, int RA>
+__device__ __forceinline__ void dif_stages(float2 (&v)[RA]) {
+  if constexpr (L >= 2) {
+    DifStage<L, L / 2, 0, INV, R / L, 0, OFF, RA>::run(v);
+    dif_stages<R, L / 2, INV, OFF, RA>(v);
+  }
+}
+
+template <int R, bool INV, int OFF, int RA>
+__device__ __forceinline__ void dft_reg(float2 (&v)[RA]) {
+  if constexpr (R >= 2) {
+    dif_stages<R, R, INV, OFF, RA>(v);
+    // undo bit reversal by renaming registers
+    float2 t[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) t[i] = v[OFF + i];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[OFF + bitrev<R>(i)] = t[i];
+  }
+}
+
+// ---------------------------------------------------------------- plans
+// Radix sequence per length. RMAX registers per thread, T = N / RMAX threads per
+// vector; in pass p each thread runs RMAX / R_p butterflies. Symmetric plans
+// (first radix == last radix) let two transforms chain in registers.
+template <int N>
+struct Plan;
+#define DOE_PLAN(NN, NP_, R0, R1, R2)                           \
+  template <>                                                   \
+  struct Plan<NN> {                                             \
+    static constexpr int NP = NP_;                              \
+    static constexpr int r0 = R0, r1 = R1, r2 = R2;             \
+    static constexpr int RMAX = (R0 > R1 ? (R0 > R2 ? R0 : R2) : (R1 > R2 ? R1 : R2)); \
+    static constexpr int T = NN / RMAX;                         \
+    static constexpr __host__ __device__ int radix(int p) { return p == 0 ? R0 : (p == 1 ? R1 : R2); } \
+  };
+DOE_PLAN(1, 1, 1, 1, 1)
+DOE_PLAN(2, 1, 2, 1, 1)
+DOE_PLAN(4, 1, 4, 1, 1)
+DOE_PLAN(8, 1, 8, 1, 1)
+DOE_PLAN(16, 1, 16, 1, 1)
+DOE_PLAN(32, 1, 32, 1, 1)
+DOE_PLAN(64, 2, 8, 8, 1)
+DOE_PLAN(128, 2, 16, 8, 1)
+DOE_PLAN(256, 2, 16, 16, 1)
+DOE_PLAN(512, 3, 8, 8, 8)
+DOE_PLAN(1024, 2, 32, 32, 1)
+DOE_PLAN(2048, 3, 16, 8, 16)
+DOE_PLAN(4096, 3, 16, 16, 16)
+DOE_PLAN(8192, 3, 32, 8, 32)
+#undef DOE_PLAN
+
+template <int N>
+constexpr int plan_radix(int p) {
+  return Plan<N>::radix(p);
+}
+template <int N, int P>
+struct PassNs {  // product of the radices before pass P
+  static constexpr int value = PassNs<N, P - 1>::value * Plan<N>::radix(P - 1);
+};
+template <int N>
+struct PassNs<N, 0> {
+  static constexpr int value = 1;
+};
+
+template <int N>
+constexpr int last_radix() {
+  return Plan<N>::radix(Plan<N>::NP - 1);
+}
+template <int N>
+constexpr bool plan_symmetric() {
+  return Plan<N>::radix(0) == last_radix<N>();
+}
+
+// Padded shared-memory index: one spare slot every 32 complex values keeps the
+// stride-R Stockham writes of the early passes free of bank conflicts.
+__device__ __forceinline__ int spad(int x) { return x + (x >> 5); }
+template <int N>
+constexpr int padded_len() {
+  return N + N / 32 + 1;
+}
+
+// Vector accessor used for the shared-memory exchanges. Row kernels place each
+// vector contiguously (stride 1, vector pitch NPAD); column kernels interleave C
+// vectors (element-major, element stride C).
+struct SmemVec {
+  float2* base;
+  int estride;  // distance between consecutive elements (1 or C)
+  int off;      // vector offset inside an interleaved tile (column kernels)
+  __device__ __forceinline__ float2& at(int e) const { return base[spad(e * estride + off)]; }
+};
+
+// ---------------------------------------------------------------- one pass
+// Apply twiddles W_{Ns R}^{r k} and the radix-R DFT for butterfly slot BI of pass P.
+template <int N, int P, bool INV, int BI>
+__device__ __forceinline__ void pass_bfly(float2 (&v)[Plan<N>::RMAX], int t, const float2* __restrict__ tw) {
+  constexpr int R = Plan<N>::radix(P);
+  constexpr int RMAX = Plan<N>::RMAX;
+  constexpr int T = Plan<N>::T;
+  constexpr int NS = PassNs<N, P>::value;
+  if constexpr (BI < RMAX / R) {
+    if constexpr (NS > 1) {
+      const int j = t + BI * T;
+      const int k = j % NS;
+      constexpr int STEP = N / (NS * R);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 w = __ldg(&tw[r * k * STEP]);
+        v[BI * R + r] = INV ? cmulc(v[BI * R + r], w) : cmul(v[BI * R + r], w);
+      }
+    }
+    dft_reg<R, INV, BI * R>(v);
+    pass_bfly<N, P, INV, BI + 1>(v, t, tw);
+  }
+}
+
+template <int N, int P, bool INV>
+__device__ __forceinline__ void pass_compute(float2 (&v)[Plan<N>::RMAX], int t, const float2* __restrict__ tw) {
+  pass_bfly<N, P, INV, 0>(v, t, tw);
+}
+
+// Write pass-P outputs to shared memory at their Stockham positions.
+template <int N, int P>
+__device__ __forceinline__ void pass_store(const float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s) {
+  constexpr int R = Plan<N>::radix(P);
+  constexpr int RMAX = Plan<N>::RMAX;
+  constexpr int T = Plan<N>::T;
+  constexpr int NS = PassNs<N, P>::value;
+#pragma unroll
+  for (int b = 0; b < RMAX / R; ++b) {
+    const int j = t + b * T;
+    const int d = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+    for (int r = 0; r < R; ++r) s.at(d + r * NS) = v[b * R + r];
+  }
+}
+
+// Read pass-P inputs from shared memory (element j + r N/R for butterfly j).
+template <int N, int P>
+__device__ __forceinline__ void pass_load(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s) {
+  constexpr int R = Plan<N>::radix(P);
+  constexpr int RMAX = Plan<N>::RMAX;
+  constexpr int T = Plan<N>::T;
+#pragma unroll
+  for (int b = 0; b < RMAX / R; ++b) {
+    const int j = t + b * T;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b * R + r] = s.at(j + r * (N / R));
+  }
+}
+
+// Element index held by register slot (b, r) before pass P (input layout).
+template <int N, int P>
+__device__ __forceinline__ int in_elem(int t, int slot) {
+  constexpr int R = Plan<N>::radix(P);
+  const int b = slot / R, r = slot % R;
+  return t + b * Plan<N>::T + r * (N / R);
+}
+// Element index held by slot after the last pass (natural-order output layout).
+template <int N>
+__device__ __forceinline__ int out_elem(int t, int slot) {
+  constexpr int R = last_radix<N>();
+  const int b = slot / R, r = slot % R;
+  return t + b * Plan<N>::T + r * (N / R);
+}
+
+// Full transform: registers hold the pass-0 input layout on entry and the
+// natural-order output layout on return. `sync` is a block or warp barrier.
+template <int N, bool INV, int P = 0, class Sync>
+__device__ __forceinline__ void fft_run(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s,
+                                        const float2* __restrict__ tw, Sync sync) {
+  pass_compute<N, P, INV>(v, t, tw);
+  if constexpr (P + 1 < Plan<N>::NP) {
+    sync();  // everyone finished reading the previous contents of s
+    pass_store<N, P>(v, t, s);
+    sync();
+    pass_load<N, P + 1>(v, t, s);
+    fft_run<N, INV, P + 1>(v, t, s, tw, sync);
+  }
+}
+
+// Re-layout registers from the output layout to the pass-0 input layout (only
+// needed for asymmetric plans when two transforms are chained).
+template <int N, class Sync>
+__device__ __forceinline__ void relayout_out_to_in(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s, Sync sync) {
+  if constexpr (!plan_symmetric<N>()) {
+    constexpr int RMAX = Plan<N>::RMAX;
+    sync();
+#pragma unroll
+    for (int q = 0; q < RMAX; ++q) s.at(out_elem<N>(t, q)) = v[q];
+    sync();
+#pragma unroll
+    for (int q = 0; q < RMAX; ++q) v[q] = s.at(in_elem<N, 0>(t, q));
+  }
+}
+
+}  // namespace doe

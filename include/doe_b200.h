@@ -1,0 +1,108 @@
+/*
+ * doe_b200.h -- C ABI of the B200 engine for the propagate-and-retrieve path of
+ * Ziggyware/DiffractiveOpticalElement (a plain-JavaScript optics toolkit).
+ *
+ * The reference exposes ES-module functions over ComplexField objects whose data
+ * are split Float64Array planes (re, im), row-major, idx = x + y*nx, optical axis
+ * at the array centre (src/field.js:8-16). Each entry point below replaces one of
+ * those functions (cited as file:line inside the reference project) and takes the
+ * same planes as plain `double*` buffers owned by the caller. A Node N-API addon,
+ * Python ctypes, or any C caller binds these symbols directly; no C++ or torch
+ * types appear in any signature.
+ *
+ * Conventions
+ *   - Every function returns a doe_status; DOE_OK is 0. On failure the message of
+ *     the failing call is available from doe_last_error(ctx) and uses the
+ *     reference's wording where the reference throws for the same condition.
+ *   - Host-buffer entry points ("doe_*" without the _dev suffix) are synchronous:
+ *     they copy the planes to HBM, run the CUDA kernels, copy results back and
+ *     return when the results are in the caller's buffers. Page-locked buffers
+ *     (doe_host_alloc) make those copies run at full PCIe rate.
+ *   - Device entry points (suffix _dev) take device pointers to complex64
+ *     (interleaved float2) planes already resident in HBM and are asynchronous on
+ *     the context's stream (doe_ctx_stream / doe_ctx_synchronize).
+ *   - A context owns one CUDA stream and its scratch memory; it is not
+ *     thread-safe. Use one context per host thread.
+ *   - Arithmetic: FP32 transforms and pointwise maths; FP64 for the angular-
+ *     spectrum phase argument (reduced mod 2*pi before FP32 sincos) and for every
+ *     power / efficiency / error / weight-normalisation reduction.
+ *   - Grids: power-of-two nx, ny in [1, 8192] (the reference accepts any power of
+ *     two; larger axes return DOE_ERR_UNSUPPORTED).
+ */
+#ifndef DOE_B200_H
+#define DOE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DOE_B200_ABI_VERSION 1
+
+typedef struct doe_ctx doe_ctx;
+
+typedef enum doe_status {
+  DOE_OK = 0,
+  DOE_ERR_NOT_POW2 = 1,      /* src/field.js:30-32, src/fft.js:88 */
+  DOE_ERR_SIZE_MISMATCH = 2, /* src/fft.js:149-151, src/field.js:78-80 */
+  DOE_ERR_BAD_ARG = 3,       /* e.g. src/propagate.js:248-250, src/doe.js:564 */
+  DOE_ERR_CUDA = 4,          /* a CUDA runtime call failed */
+  DOE_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  DOE_ERR_UNSUPPORTED = 6,   /* outside the engine's supported range */
+  DOE_ERR_NO_DEVICE = 7      /* no CUDA device / library not usable */
+} doe_status;
+
+/* ------------------------------------------------------------ context */
+int doe_abi_version(void);
+int doe_ctx_create(int device, doe_ctx** out);
+void doe_ctx_destroy(doe_ctx* ctx);
+const char* doe_last_error(const doe_ctx* ctx);
+void* doe_ctx_stream(doe_ctx* ctx); /* the context's cudaStream_t */
+int doe_ctx_synchronize(doe_ctx* ctx);
+/* Page-locked host allocation for fast host<->device copies. */
+int doe_host_alloc(doe_ctx* ctx, void** ptr, unsigned long long bytes);
+int doe_host_free(doe_ctx* ctx, void* ptr);
+
+/* ------------------------------------------------------------ transforms */
+/* fft2d(re, im, nx, ny, inverse) -- src/fft.js:148-154. In place; forward
+ * unscaled, inverse scaled by 1/(nx*ny). */
+int doe_fft2d(doe_ctx* ctx, double* re, double* im, int nx, int ny, int inverse);
+
+/* angularSpectrumTransferFunction -- src/propagate.js:57-102. Writes the centred
+ * transfer function and the propagating fraction (entries with w > 0.5). */
+int doe_asm_transfer(doe_ctx* ctx, int nx, int ny, double dx, double dy, double lambda,
+                     double z, int band_limit, int evanescent, double soft_edge,
+                     double* h_re, double* h_im, double* propagating_fraction);
+
+/* propagateAngularSpectrumInPlace -- src/propagate.js:112-133 (z may be negative;
+ * z == 0 leaves the field untouched). propagateAngularSpectrum (:105-109) is the
+ * same call on a copy. */
+int doe_asm(doe_ctx* ctx, double* re, double* im, int nx, int ny, double dx, double dy,
+            double lambda, double z, int band_limit, int evanescent, double soft_edge);
+
+/* focusSweep -- src/propagate.js:427-434: one input field propagated to nz
+ * distances; out_re/out_im hold nz consecutive planes. */
+int doe_asm_sweep(doe_ctx* ctx, const double* re, const double* im, int nx, int ny,
+                  double dx, double dy, double lambda, const double* z, int nz,
+                  int band_limit, int evanescent, double soft_edge, double* out_re,
+                  double* out_im);
+
+/* focalPlaneSpectrum -- src/propagate.js:342-374. Output pitch in out_d[0..1]. */
+int doe_focal_plane(doe_ctx* ctx, const double* re, const double* im, int nx, int ny,
+                    double dx, double dy, double lambda, double f, double* out_re,
+                    double* out_im, double* out_d);
+
+/* ------------------------------------------------------------ device-resident */
+/* Batched 2-D FFT of nplanes complex64 planes in place (device pointer). */
+int doe_fft2d_dev(doe_ctx* ctx, void* d_planes, int nx, int ny, int nplanes, int inverse);
+
+/* Batched focus sweep on device-resident complex64 fields: field f (of nfields)
+ * with wavelength lambda[f] is propagated to z[f*nz + k] for k < nz and written
+ * to plane f*nz + k of d_out. lambda and z are host arrays. */
+int doe_asm_sweep_dev(doe_ctx* ctx, const void* d_fields, int nfields, int nx, int ny,
+                      double dx, double dy, const double* lambda, const double* z, int nz,
+                      int band_limit, int evanescent, double soft_edge, void* d_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOE_B200_H */

@@ -1,0 +1,877 @@
+/*
+ * doe_oracle.c -- FP64 CPU restatement of the reference's propagate-and-retrieve
+ * path. TEST INFRASTRUCTURE ONLY: the parity checker and timed CPU baseline.
+ * The product (diffractiveopticalelement_b200) never links or calls it.
+ *
+ * Build without -ffast-math (see oracle/Makefile): operation order matters.
+ * Each function cites the reference file:line (paths inside the reference
+ * project) whose loop it restates.
+ */
+#include "doe_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Twiddles: src/fft.js:29-48. One table per power-of-two length, built once
+ * for every length up to 2^MAX_LOG2 (the reference caches them lazily; the
+ * values are identical). */
+#define MAX_LOG2 16
+static double* g_tw_cos[MAX_LOG2 + 1];
+static double* g_tw_sin[MAX_LOG2 + 1];
+static pthread_once_t g_tw_once = PTHREAD_ONCE_INIT;
+
+static void build_twiddles(void) {
+  for (int lg = 1; lg <= MAX_LOG2; lg++) {
+    int n = 1 << lg;
+    int half = n >> 1;
+    g_tw_cos[lg] = (double*)malloc(sizeof(double) * half);
+    g_tw_sin[lg] = (double*)malloc(sizeof(double) * half);
+    for (int k = 0; k < half; k++) {
+      double a = (-2.0 * M_PI * (double)k) / (double)n;
+      g_tw_cos[lg][k] = cos(a);
+      g_tw_sin[lg][k] = sin(a);
+    }
+  }
+}
+
+static int is_pow2(long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+/* src/fft.js:86-139 */
+int orc_fft1d(double* re, double* im, int n, long stride, long offset, int inverse) {
+  if (n <= 1) return 0;
+  if (!is_pow2(n) || n > (1 << MAX_LOG2)) return -1;
+  pthread_once(&g_tw_once, build_twiddles);
+  /* bit-reversal permutation (src/fft.js:91-105) */
+  for (int i = 1, j = 0; i < n; i++) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      long ia = offset + (long)i * stride;
+      long ja = offset + (long)j * stride;
+      double tr = re[ia];
+      re[ia] = re[ja];
+      re[ja] = tr;
+      double ti = im[ia];
+      im[ia] = im[ja];
+      im[ja] = ti;
+    }
+  }
+  /* butterflies (src/fft.js:108-129) */
+  for (int len = 2, lg = 1; len <= n; len <<= 1, lg++) {
+    int half = len >> 1;
+    const double* cs = g_tw_cos[lg];
+    const double* sn = g_tw_sin[lg];
+    for (int base = 0; base < n; base += len) {
+      long b0 = offset + (long)base * stride;
+      for (int k = 0; k < half; k++) {
+        double wr = cs[k];
+        double wi = inverse ? -sn[k] : sn[k];
+        long p = b0 + (long)k * stride;
+        long q = p + (long)half * stride;
+        double xr = re[q];
+        double xi = im[q];
+        double tr = xr * wr - xi * wi;
+        double ti = xr * wi + xi * wr;
+        re[q] = re[p] - tr;
+        im[q] = im[p] - ti;
+        re[p] += tr;
+        im[p] += ti;
+      }
+    }
+  }
+  /* per-pass 1/n (src/fft.js:131-138) */
+  if (inverse) {
+    double s = 1.0 / (double)n;
+    for (int i = 0; i < n; i++) {
+      long p = offset + (long)i * stride;
+      re[p] *= s;
+      im[p] *= s;
+    }
+  }
+  return 0;
+}
+
+/* src/fft.js:148-154 */
+int orc_fft2d(double* re, double* im, int nx, int ny, int inverse) {
+  if (!is_pow2(nx) || !is_pow2(ny)) return -1;
+  for (int y = 0; y < ny; y++)
+    if (orc_fft1d(re, im, nx, 1, (long)y * nx, inverse)) return -1;
+  for (int x = 0; x < nx; x++)
+    if (orc_fft1d(re, im, ny, nx, x, inverse)) return -1;
+  return 0;
+}
+
+/* src/fft.js:170-181 */
+static void fftshift1d(double* arr, int n, int shift, long stride, long offset) {
+  int m = n >> 1;
+  int d = shift ? m : n - m;
+  for (int i = 0; i < m; i++) {
+    long a = offset + (long)i * stride;
+    long b = offset + (long)((i + d) % n) * stride;
+    double t = arr[a];
+    arr[a] = arr[b];
+    arr[b] = t;
+  }
+}
+
+/* src/fft.js:188-202 */
+void orc_fftshift2d(double* re, double* im, int nx, int ny, int shift) {
+  for (int y = 0; y < ny; y++) {
+    long row = (long)y * nx;
+    fftshift1d(re, nx, shift, 1, row);
+    if (im) fftshift1d(im, nx, shift, 1, row);
+  }
+  for (int x = 0; x < nx; x++) {
+    fftshift1d(re, ny, shift, nx, x);
+    if (im) fftshift1d(im, ny, shift, nx, x);
+  }
+}
+
+/* src/fft.js:208-237 */
+void orc_dft2d_naive(const double* re, const double* im, int nx, int ny, int inverse,
+                     double* out_re, double* out_im) {
+  double sign = inverse ? 1.0 : -1.0;
+  double scale = inverse ? 1.0 / (double)(nx * ny) : 1.0;
+  for (int ky = 0; ky < ny; ky++) {
+    for (int kx = 0; kx < nx; kx++) {
+      double sr = 0, si = 0;
+      for (int y = 0; y < ny; y++) {
+        double ay = (sign * 2.0 * M_PI * ky * y) / ny;
+        double cy = cos(ay), sy = sin(ay);
+        for (int x = 0; x < nx; x++) {
+          double ax = (sign * 2.0 * M_PI * kx * x) / nx;
+          double c = cos(ax) * cy - sin(ax) * sy;
+          double s = sin(ax) * cy + cos(ax) * sy;
+          double vr = re[x + y * nx];
+          double vi = im[x + y * nx];
+          sr += vr * c - vi * s;
+          si += vr * s + vi * c;
+        }
+      }
+      long o = kx + (long)ky * nx;
+      out_re[o] = sr * scale;
+      out_im[o] = si * scale;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* src/propagate.js:38-42 */
+static double soft_window(double v, double lim, double inner) {
+  if (v <= inner) return 1;
+  if (v >= lim) return 0;
+  return 0.5 * (1 + cos((M_PI * (v - inner)) / (lim - inner)));
+}
+
+/* src/propagate.js:48-51 */
+double orc_local_frequency_limit(int n, double d, double lambda, double z) {
+  double df = 1.0 / (n * d);
+  return 1.0 / (lambda * sqrt(pow(2 * df * z, 2) + 1));
+}
+
+/* src/propagate.js:57-102 */
+double orc_asm_transfer(int nx, int ny, double dx, double dy, double lambda, double z,
+                        int band_limit, int evanescent, double soft_edge, double* re,
+                        double* im) {
+  double dfx = 1.0 / (nx * dx);
+  double dfy = 1.0 / (ny * dy);
+  double invL2 = 1.0 / (lambda * lambda);
+  double fxLim = band_limit ? orc_local_frequency_limit(nx, dx, lambda, z) : INFINITY;
+  double fyLim = band_limit ? orc_local_frequency_limit(ny, dy, lambda, z) : INFINITY;
+  double fxn = 1.0 / (2 * dx);
+  double fyn = 1.0 / (2 * dy);
+  long propagating = 0;
+  for (int j = 0; j < ny; j++) {
+    double fy = (j - ny / 2.0) * dfy;
+    double limY = fmin(fyLim, fyn);
+    double wy = isinf(fyLim) ? 1 : soft_window(fabs(fy), limY, limY * (1 - soft_edge));
+    for (int i = 0; i < nx; i++) {
+      double fx = (i - nx / 2.0) * dfx;
+      double limX = fmin(fxLim, fxn);
+      double wx = isinf(fxLim) ? 1 : soft_window(fabs(fx), limX, limX * (1 - soft_edge));
+      double arg = invL2 - fx * fx - fy * fy;
+      long k = i + (long)j * nx;
+      if (arg >= 0) {
+        double phase = 2 * M_PI * z * sqrt(arg);
+        double w = wx * wy;
+        re[k] = w * cos(phase);
+        im[k] = w * sin(phase);
+        if (w > 0.5) propagating++;
+      } else if (evanescent) {
+        re[k] = 0;
+        im[k] = 0;
+      } else {
+        double w = wx * wy;
+        double phase = 2 * M_PI * z * sqrt(-arg);
+        re[k] = w * cos(phase);
+        im[k] = w * sin(phase);
+        propagating++;
+      }
+    }
+  }
+  return (double)propagating / (double)((long)nx * ny);
+}
+
+/* src/propagate.js:112-133 */
+void orc_asm_inplace(double* re, double* im, int nx, int ny, double dx, double dy,
+                     double lambda, double z, int band_limit, int evanescent,
+                     double soft_edge) {
+  if (z == 0) return;
+  long n = (long)nx * ny;
+  orc_fftshift2d(re, im, nx, ny, 0);
+  orc_fft2d(re, im, nx, ny, 0);
+  orc_fftshift2d(re, im, nx, ny, 1);
+  double* hr = (double*)malloc(sizeof(double) * n);
+  double* hi = (double*)malloc(sizeof(double) * n);
+  orc_asm_transfer(nx, ny, dx, dy, lambda, z, band_limit, evanescent, soft_edge, hr, hi);
+  for (long k = 0; k < n; k++) {
+    double ur = re[k], ui = im[k];
+    re[k] = ur * hr[k] - ui * hi[k];
+    im[k] = ur * hi[k] + ui * hr[k];
+  }
+  free(hr);
+  free(hi);
+  orc_fftshift2d(re, im, nx, ny, 0);
+  orc_fft2d(re, im, nx, ny, 1);
+  orc_fftshift2d(re, im, nx, ny, 1);
+}
+
+/* src/propagate.js:342-374 */
+void orc_focal_plane(const double* in_re, const double* in_im, int nx, int ny, double dx,
+                     double dy, double lambda, double f, double* re, double* im,
+                     double* out_d) {
+  long n = (long)nx * ny;
+  memcpy(re, in_re, sizeof(double) * n);
+  memcpy(im, in_im, sizeof(double) * n);
+  orc_fftshift2d(re, im, nx, ny, 0);
+  orc_fft2d(re, im, nx, ny, 0);
+  orc_fftshift2d(re, im, nx, ny, 1);
+  double dux = (lambda * f) / (nx * dx);
+  double duy = (lambda * f) / (ny * dy);
+  double amp0 = (dx * dy) / (lambda * f);
+  for (int j = 0; j < ny; j++) {
+    double v = (j - ny / 2.0) * duy;
+    for (int i = 0; i < nx; i++) {
+      double u = (i - nx / 2.0) * dux;
+      long idx = i + (long)j * nx;
+      double q = (M_PI * (u * u + v * v)) / (lambda * f) - M_PI / 2;
+      double c = amp0 * cos(q);
+      double s = amp0 * sin(q);
+      double ur = re[idx], ui = im[idx];
+      re[idx] = ur * c - ui * s;
+      im[idx] = ur * s + ui * c;
+    }
+  }
+  if (out_d) {
+    out_d[0] = dux;
+    out_d[1] = duy;
+  }
+}
+
+/* src/propagate.js:155-239 */
+void orc_fresnel_fft(const double* in_re, const double* in_im, int nx, int ny, double dx,
+                     double dy, double lambda, double z, double* re, double* im,
+                     double* out_d) {
+  double az = fabs(z);
+  double k = (2 * M_PI) / lambda;
+  double dux = (lambda * az) / (nx * dx);
+  double duy = (lambda * az) / (ny * dy);
+  for (int j = 0; j < ny; j++) {
+    double y = (j - ny / 2.0) * dy;
+    for (int i = 0; i < nx; i++) {
+      double x = (i - nx / 2.0) * dx;
+      double q = (M_PI * (x * x + y * y)) / (lambda * az);
+      double c = ((i + j) % 2) ? -cos(q) : cos(q);
+      double s = ((i + j) % 2) ? -sin(q) : sin(q);
+      long idx = i + (long)j * nx;
+      double ur = in_re[idx], ui = in_im[idx];
+      re[idx] = ur * c - ui * s;
+      im[idx] = ur * s + ui * c;
+    }
+  }
+  orc_fft2d(re, im, nx, ny, 0);
+  double amp = (dx * dy) / (lambda * az);
+  double kz = k * z - (M_PI * (nx + ny)) / 2;
+  double ckz = cos(kz), skz = sin(kz);
+  double pr = amp * skz;
+  double pj = -amp * ckz;
+  for (int j = 0; j < ny; j++) {
+    double v = ((j - ny / 2.0) * dy) * 0 + (j - ny / 2.0) * duy;
+    for (int i = 0; i < nx; i++) {
+      double u = (i - nx / 2.0) * dux;
+      double q = (M_PI * (u * u + v * v)) / (lambda * az);
+      double c = ((i + j) % 2) ? -cos(q) : cos(q);
+      double s = ((i + j) % 2) ? -sin(q) : sin(q);
+      long idx = i + (long)j * nx;
+      double ur = re[idx], ui = im[idx];
+      double tr = ur * pr - ui * pj;
+      double ti = ur * pj + ui * pr;
+      re[idx] = tr * c - ti * s;
+      im[idx] = tr * s + ti * c;
+    }
+  }
+  if (out_d) {
+    out_d[0] = dux;
+    out_d[1] = duy;
+  }
+}
+
+/* src/propagate.js:246-316 */
+void orc_fresnel_fft_inverse(const double* in_re, const double* in_im, int nx, int ny,
+                             double dux, double duy, double lambda, double z, double dx,
+                             double dy, double* re, double* im) {
+  double az = fabs(z);
+  double k = (2 * M_PI) / lambda;
+  for (int j = 0; j < ny; j++) {
+    double v = (j - ny / 2.0) * duy;
+    for (int i = 0; i < nx; i++) {
+      double u = (i - nx / 2.0) * dux;
+      double q = (M_PI * (u * u + v * v)) / (lambda * az);
+      double sg = ((i + j) % 2) ? -1 : 1;
+      double c = sg * cos(q);
+      double s = -sg * sin(q);
+      long idx = i + (long)j * nx;
+      double ur = in_re[idx], ui = in_im[idx];
+      re[idx] = ur * c - ui * s;
+      im[idx] = ur * s + ui * c;
+    }
+  }
+  orc_fft2d(re, im, nx, ny, 1);
+  double amp = (lambda * az) / (dx * dy);
+  double kg = k * z - (M_PI * (nx + ny)) / 2 - M_PI / 2;
+  double cg = cos(kg), sg2 = sin(kg);
+  double pr = amp * cg;
+  double pj = -amp * sg2;
+  for (int j = 0; j < ny; j++) {
+    double y = (j - ny / 2.0) * dy;
+    for (int i = 0; i < nx; i++) {
+      double x = (i - nx / 2.0) * dx;
+      double q = (M_PI * (x * x + y * y)) / (lambda * az);
+      double sg = ((i + j) % 2) ? -1 : 1;
+      double c = sg * cos(q);
+      double s = -sg * sin(q);
+      long idx = i + (long)j * nx;
+      double ur = re[idx], ui = im[idx];
+      double tr = ur * pr - ui * pj;
+      double ti = ur * pj + ui * pr;
+      re[idx] = tr * c - ti * s;
+      im[idx] = tr * s + ti * c;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* src/field.js:516-536 */
+void orc_disc_mask(int nx, int ny, double dx, double dy, double radius, double soft,
+                   double cx, double cy, double* m) {
+  for (int j = 0; j < ny; j++) {
+    double y = (j - ny / 2.0) * dy - cy;
+    for (int i = 0; i < nx; i++) {
+      double x = (i - nx / 2.0) * dx - cx;
+      double r = hypot(x, y);
+      double v;
+      if (soft > 0) {
+        v = r <= radius - soft ? 1
+            : r >= radius      ? 0
+                               : 0.5 * (1 + cos((M_PI * (r - radius + soft)) / soft));
+      } else {
+        v = r <= radius ? 1 : 0;
+      }
+      m[i + (long)j * nx] = v;
+    }
+  }
+}
+
+/* src/field.js:554-558 */
+static double edge_fn(double x, double half, double soft) {
+  if (x <= half - soft) return 1;
+  if (x >= half) return 0;
+  return 0.5 * (1 + cos((M_PI * (x - half + soft)) / soft));
+}
+
+/* src/field.js:539-552 */
+void orc_rect_mask(int nx, int ny, double dx, double dy, double width, double height,
+                   double soft, double* m) {
+  for (int j = 0; j < ny; j++) {
+    double y = fabs((j - ny / 2.0) * dy);
+    for (int i = 0; i < nx; i++) {
+      double x = fabs((i - nx / 2.0) * dx);
+      double fx = soft > 0 ? edge_fn(x, width / 2, soft) : (x <= width / 2 ? 1 : 0);
+      double fy = soft > 0 ? edge_fn(y, height / 2, soft) : (y <= height / 2 ? 1 : 0);
+      m[i + (long)j * nx] = fx * fy;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* src/doe.js:65-75: `seed >>> 0 || 1` then xorshift32 (13, 17, 5). */
+uint32_t orc_rng_seed(double seed) {
+  /* ToUint32: truncate toward zero, modulo 2^32. */
+  double t = trunc(seed);
+  double m = fmod(t, 4294967296.0);
+  if (m < 0) m += 4294967296.0;
+  uint32_t s = (uint32_t)m;
+  return s ? s : 1u;
+}
+
+double orc_rng_next(uint32_t* state) {
+  uint32_t s = *state;
+  s ^= s << 13;
+  s ^= s >> 17;
+  s ^= s << 5;
+  *state = s;
+  return (double)s / 4294967296.0;
+}
+
+/* src/doe.js:81-86 */
+void orc_random_phase(int nx, int ny, double seed, double* p) {
+  uint32_t st = orc_rng_seed(seed);
+  long n = (long)nx * ny;
+  for (long k = 0; k < n; k++) p[k] = (orc_rng_next(&st) * 2 - 1) * M_PI;
+}
+
+/* ------------------------------------------------------------------ */
+/* src/doe.js:327-437 */
+int orc_gerchberg_saxton(const double* illumination, const double* targetAmp,
+                         const orc_design_opts* o, orc_design_result* r) {
+  int nx = o->nx, ny = o->ny;
+  long n = (long)nx * ny;
+  double dx = o->dx, dy = o->dy;
+  const double* roi = o->roi;
+  const double* weights = o->weights;
+  double* re = (double*)malloc(sizeof(double) * n);
+  double* im = (double*)malloc(sizeof(double) * n);
+  double* amp = (double*)malloc(sizeof(double) * n);
+  if (!re || !im || !amp) return -2;
+  double* phase = r->phase;
+  if (o->init_phase) {
+    if (phase != o->init_phase) memcpy(phase, o->init_phase, sizeof(double) * n);
+  } else {
+    memset(phase, 0, sizeof(double) * n);
+  }
+  for (int it = 0; it < o->iterations; it++) {
+    /* forward: setAmplitudePhase + copyFrom + ASM(+z) (src/doe.js:350-352) */
+    for (long k = 0; k < n; k++) {
+      re[k] = illumination[k] * cos(phase[k]);
+      im[k] = illumination[k] * sin(phase[k]);
+    }
+    orc_asm_inplace(re, im, nx, ny, dx, dy, o->lambda, o->z, 0, 1, 0.02);
+    /* measurement (src/doe.js:355-377) */
+    double errNum = 0, errDen = 0, inRoi = 0, total = 0;
+    for (long k = 0; k < n; k++) {
+      double a = hypot(re[k], im[k]);
+      double i2 = a * a;
+      amp[k] = a;
+      total += i2;
+      double m = roi ? roi[k] : 1;
+      double t = targetAmp[k] * (weights ? weights[k] : 1);
+      if (m > 0) {
+        inRoi += i2 * m;
+        if (t > 0 || i2 > 0) {
+          double d = a * m - t * m;
+          errNum += d * d;
+          errDen += t * t;
+        }
+      }
+    }
+    if (r->error) r->error[it] = errDen > 0 ? sqrt(errNum / errDen) : 0;
+    if (r->efficiency) r->efficiency[it] = total > 0 ? (inRoi * dx * dy) / (total * dx * dy) : 0;
+    /* constraint (src/doe.js:380-397) */
+    double fb = it >= o->escape ? o->feedback : 0;
+    for (long k = 0; k < n; k++) {
+      double m = roi ? roi[k] : 1;
+      double t = targetAmp[k] * (weights ? weights[k] : 1);
+      double a = amp[k];
+      double newAmp;
+      if (m > 0) {
+        newAmp = t;
+        if (fb > 0 && a > 0) newAmp = t + fb * (a - t);
+      } else {
+        newAmp = a * (1 - fb) + fb * a;
+      }
+      if (a > 0) {
+        double s = newAmp / a;
+        re[k] *= s;
+        im[k] *= s;
+      }
+    }
+    /* back-propagate, keep the phase (src/doe.js:400-410) */
+    orc_asm_inplace(re, im, nx, ny, dx, dy, o->lambda, -o->z, 0, 1, 0.02);
+    for (long k = 0; k < n; k++) phase[k] = atan2(im[k], re[k]);
+  }
+  /* final honest forward pass (src/doe.js:418-426) */
+  for (long k = 0; k < n; k++) {
+    re[k] = illumination[k] * cos(phase[k]);
+    im[k] = illumination[k] * sin(phase[k]);
+  }
+  orc_asm_inplace(re, im, nx, ny, dx, dy, o->lambda, o->z, 0, 1, 0.02);
+  for (long k = 0; k < n; k++) {
+    double a = hypot(re[k], im[k]);
+    if (r->amplitude) r->amplitude[k] = a;
+    if (r->intensity) r->intensity[k] = a * a;
+  }
+  free(re);
+  free(im);
+  free(amp);
+  return 0;
+}
+
+/* src/doe.js:639-730 */
+int orc_fourier_cgh(const double* illumination, const double* targetAmp,
+                    const orc_design_opts* o, orc_design_result* r) {
+  int nx = o->nx, ny = o->ny;
+  long n = (long)nx * ny;
+  const double* roi = o->roi;
+  const double* weights = o->weights;
+  double* re = (double*)malloc(sizeof(double) * n);
+  double* im = (double*)malloc(sizeof(double) * n);
+  if (!re || !im) return -2;
+  double* phase = r->phase;
+  if (o->init_phase) {
+    if (phase != o->init_phase) memcpy(phase, o->init_phase, sizeof(double) * n);
+  } else {
+    orc_random_phase(nx, ny, o->seed, phase);
+  }
+  double norm = 1.0 / sqrt((double)nx * ny);
+  for (int it = 0; it < o->iterations; it++) {
+    for (long k = 0; k < n; k++) {
+      double a = illumination[k];
+      re[k] = a * cos(phase[k]);
+      im[k] = a * sin(phase[k]);
+    }
+    orc_fftshift2d(re, im, nx, ny, 0);
+    orc_fft2d(re, im, nx, ny, 0);
+    orc_fftshift2d(re, im, nx, ny, 1);
+    for (long k = 0; k < n; k++) {
+      re[k] *= norm;
+      im[k] *= norm;
+    }
+    double errNum = 0, errDen = 0, inRoi = 0, total = 0;
+    for (long k = 0; k < n; k++) {
+      double a = hypot(re[k], im[k]);
+      if (r->amplitude) r->amplitude[k] = a;
+      if (r->intensity) r->intensity[k] = a * a;
+      total += a * a;
+      double m = roi ? roi[k] : 1;
+      double t = targetAmp[k] * (weights ? weights[k] : 1);
+      if (m > 0) {
+        inRoi += a * a * m;
+        double d = (a - t) * m;
+        errNum += d * d;
+        errDen += t * t;
+      }
+    }
+    if (r->error) r->error[it] = errDen > 0 ? sqrt(errNum / errDen) : 0;
+    if (r->efficiency) r->efficiency[it] = total > 0 ? inRoi / total : 0;
+    for (long k = 0; k < n; k++) {
+      double m = roi ? roi[k] : 1;
+      double a = hypot(re[k], im[k]);
+      double t = m > 0 ? targetAmp[k] * (weights ? weights[k] : 1) : a;
+      if (a > 0) {
+        double s = t / a;
+        re[k] *= s;
+        im[k] *= s;
+      } else {
+        re[k] = t;
+        im[k] = 0;
+      }
+    }
+    orc_fftshift2d(re, im, nx, ny, 0);
+    orc_fft2d(re, im, nx, ny, 1);
+    orc_fftshift2d(re, im, nx, ny, 1);
+    for (long k = 0; k < n; k++) {
+      re[k] *= sqrt((double)nx * ny);
+      im[k] *= sqrt((double)nx * ny);
+      phase[k] = atan2(im[k], re[k]);
+    }
+  }
+  free(re);
+  free(im);
+  return 0;
+}
+
+/* src/doe.js:455-546 */
+int orc_weighted_gs(const double* illumination, const double* targetAmp,
+                    const orc_design_opts* o, int base, orc_design_result* r) {
+  int nx = o->nx, ny = o->ny;
+  long n = (long)nx * ny;
+  const double* roi = o->roi;
+  if (o->iterations < 1) return -1; /* the reference dereferences a null result */
+  double* weights = r->weights ? r->weights : (double*)malloc(sizeof(double) * n);
+  double* cur_phase = (double*)malloc(sizeof(double) * n);
+  double* amp = (double*)malloc(sizeof(double) * n);
+  double* inten = (double*)malloc(sizeof(double) * n);
+  double* eff = (double*)malloc(sizeof(double));
+  double* best_phase = (double*)malloc(sizeof(double) * n);
+  double* best_amp = (double*)malloc(sizeof(double) * n);
+  double* best_int = (double*)malloc(sizeof(double) * n);
+  if (!weights || !cur_phase || !amp || !inten || !eff || !best_phase || !best_amp || !best_int)
+    return -2;
+  for (long k = 0; k < n; k++) weights[k] = ((roi ? roi[k] : 1) > 0) ? 1 : 0;
+  double bestRmse = INFINITY;
+  int have_best = 0;
+  double beta = o->beta;
+  for (int it = 0; it < o->iterations; it++) {
+    orc_design_opts so = *o;
+    so.weights = weights;
+    so.iterations = 1;
+    so.init_phase = it > 0 ? cur_phase : o->init_phase;
+    orc_design_result sr;
+    memset(&sr, 0, sizeof(sr));
+    sr.phase = cur_phase;
+    sr.amplitude = amp;
+    sr.intensity = inten;
+    sr.efficiency = eff;
+    int rc = base == 1 ? orc_fourier_cgh(illumination, targetAmp, &so, &sr)
+                       : orc_gerchberg_saxton(illumination, targetAmp, &so, &sr);
+    if (rc) return rc;
+    /* unweighted ROI RMSE and best-iterate snapshot (src/doe.js:489-504) */
+    double num = 0, den = 0;
+    for (long k = 0; k < n; k++) {
+      if ((roi ? roi[k] : 1) <= 0) continue;
+      double d = amp[k] - targetAmp[k];
+      num += d * d;
+      den += targetAmp[k] * targetAmp[k];
+    }
+    double rmse = den > 0 ? sqrt(num / den) : 0;
+    if (rmse < bestRmse) {
+      bestRmse = rmse;
+      memcpy(best_phase, cur_phase, sizeof(double) * n);
+      memcpy(best_amp, amp, sizeof(double) * n);
+      memcpy(best_int, inten, sizeof(double) * n);
+      have_best = 1;
+    }
+    /* multiplicative weight update + renormalisation (src/doe.js:510-524) */
+    double wsum = 0, tsum = 0;
+    for (long k = 0; k < n; k++) {
+      if ((roi ? roi[k] : 1) <= 0) continue;
+      double measured = amp[k];
+      double desired = targetAmp[k];
+      double ratio = measured > 1e-30 ? desired / measured : 2;
+      weights[k] *= pow(fmin(fmax(ratio, 0.25), 4), beta);
+      weights[k] = fmin(fmax(weights[k], 1e-4), 1e4);
+      wsum += weights[k] * weights[k] * desired * desired;
+      tsum += desired * desired;
+    }
+    double nrm = wsum > 0 ? sqrt(tsum / wsum) : 1;
+    for (long k = 0; k < n; k++) weights[k] *= nrm;
+    if (r->error) r->error[it] = bestRmse;
+    if (r->efficiency) r->efficiency[it] = eff[0];
+  }
+  if (have_best) {
+    memcpy(r->phase, best_phase, sizeof(double) * n);
+    if (r->amplitude) memcpy(r->amplitude, best_amp, sizeof(double) * n);
+    if (r->intensity) memcpy(r->intensity, best_int, sizeof(double) * n);
+  } else {
+    memcpy(r->phase, cur_phase, sizeof(double) * n);
+    if (r->amplitude) memcpy(r->amplitude, amp, sizeof(double) * n);
+    if (r->intensity) memcpy(r->intensity, inten, sizeof(double) * n);
+  }
+  r->rmse = bestRmse;
+  if (!r->weights) free(weights);
+  free(cur_phase);
+  free(amp);
+  free(inten);
+  free(eff);
+  free(best_phase);
+  free(best_amp);
+  free(best_int);
+  return 0;
+}
+
+/* src/doe.js:557-626 */
+int orc_gs_multiplane(const double* illumination, int nplanes, const double* zs,
+                      const double* target_amp, const double* roi_all,
+                      const double* weight, const orc_design_opts* o, double* phase,
+                      double* error, double* efficiency, double* per_plane_error) {
+  int nx = o->nx, ny = o->ny;
+  long n = (long)nx * ny;
+  if (nplanes == 0) return -1;
+  double* re = (double*)malloc(sizeof(double) * n);
+  double* im = (double*)malloc(sizeof(double) * n);
+  double* amps = (double*)malloc(sizeof(double) * n);
+  if (!re || !im || !amps) return -2;
+  if (o->init_phase) {
+    if (phase != o->init_phase) memcpy(phase, o->init_phase, sizeof(double) * n);
+  } else {
+    memset(phase, 0, sizeof(double) * n);
+  }
+  for (int it = 0; it < o->iterations; it++) {
+    double iterErr = 0;
+    for (int p = 0; p < nplanes; p++) {
+      double z = zs[p];
+      const double* targetAmp = target_amp + (long)p * n;
+      const double* roi = roi_all ? roi_all + (long)p * n : NULL;
+      double w = weight ? weight[p] : 1;
+      for (long k = 0; k < n; k++) {
+        re[k] = illumination[k] * cos(phase[k]);
+        im[k] = illumination[k] * sin(phase[k]);
+      }
+      orc_asm_inplace(re, im, nx, ny, o->dx, o->dy, o->lambda, z, 0, 1, 0.02);
+      double errNum = 0, errDen = 0, inRoi = 0, total = 0;
+      for (long k = 0; k < n; k++) {
+        double a = hypot(re[k], im[k]);
+        amps[k] = a;
+        double i2 = a * a;
+        total += i2;
+        double m = roi ? roi[k] : 1;
+        if (m > 0) {
+          inRoi += i2 * m;
+          double d = (a - targetAmp[k]) * m;
+          errNum += d * d;
+          errDen += targetAmp[k] * targetAmp[k];
+        }
+      }
+      (void)inRoi;
+      (void)total;
+      double e = errDen > 0 ? sqrt(errNum / errDen) : 0;
+      if (per_plane_error) per_plane_error[(long)p * o->iterations + it] = e;
+      iterErr += e * w;
+      for (long k = 0; k < n; k++) {
+        double m = roi ? roi[k] : 1;
+        double t = m > 0 ? targetAmp[k] : amps[k];
+        if (amps[k] > 0) {
+          double s = t / amps[k];
+          re[k] *= s;
+          im[k] *= s;
+        }
+      }
+      orc_asm_inplace(re, im, nx, ny, o->dx, o->dy, o->lambda, -z, 0, 1, 0.02);
+      for (long k = 0; k < n; k++) phase[k] = atan2(im[k], re[k]);
+    }
+    if (error) error[it] = iterErr / nplanes;
+    if (efficiency) efficiency[it] = 1 - iterErr / nplanes;
+  }
+  free(re);
+  free(im);
+  free(amps);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* JavaScript Math.round: round half toward +infinity. */
+static double js_round(double x) { return floor(x + 0.5); }
+
+/* src/projector.js:262-315 */
+void orc_auto_roi(const double* irr, int nx, int ny, double dilate, double soft,
+                  double threshold, double* out) {
+  long n = (long)nx * ny;
+  double mx = 0;
+  for (long k = 0; k < n; k++)
+    if (irr[k] > mx) mx = irr[k];
+  double* bin = (double*)malloc(sizeof(double) * n);
+  double* tmp = (double*)malloc(sizeof(double) * n);
+  double* dil = (double*)malloc(sizeof(double) * n);
+  for (long k = 0; k < n; k++) bin[k] = irr[k] > threshold * mx ? 1 : 0;
+  int r = (int)fmax(1, js_round(dilate));
+  for (int j = 0; j < ny; j++) {
+    for (int i = 0; i < nx; i++) {
+      double v = 0;
+      for (int d = -r; d <= r && v == 0; d++) {
+        int ii = i + d;
+        if (ii < 0 || ii >= nx) continue;
+        if (bin[ii + (long)j * nx] > 0) v = 1;
+      }
+      tmp[i + (long)j * nx] = v;
+    }
+  }
+  for (int j = 0; j < ny; j++) {
+    for (int i = 0; i < nx; i++) {
+      double v = 0;
+      for (int d = -r; d <= r && v == 0; d++) {
+        int jj = j + d;
+        if (jj < 0 || jj >= ny) continue;
+        if (tmp[i + (long)jj * nx] > 0) v = 1;
+      }
+      dil[i + (long)j * nx] = v;
+    }
+  }
+  if (soft <= 0) {
+    memcpy(out, dil, sizeof(double) * n);
+  } else {
+    int s = (int)fmax(1, js_round(soft));
+    for (int j = 0; j < ny; j++) {
+      for (int i = 0; i < nx; i++) {
+        double acc = 0;
+        int cnt = 0;
+        for (int dj = -s; dj <= s; dj++) {
+          int jj = j + dj;
+          if (jj < 0 || jj >= ny) continue;
+          for (int di = -s; di <= s; di++) {
+            int ii = i + di;
+            if (ii < 0 || ii >= nx) continue;
+            acc += dil[ii + (long)jj * nx];
+            cnt++;
+          }
+        }
+        out[i + (long)j * nx] = cnt > 0 ? acc / cnt : 0;
+      }
+    }
+  }
+  free(bin);
+  free(tmp);
+  free(dil);
+}
+
+/* src/projector.js:554-595 (rmse / efficiency / flux subset), src/metrics.js:10-18,73-84 */
+void orc_screen_metrics(const double* fre, const double* fim, int nx, int ny, double sdx,
+                        double sdy, const double* target_irr, const double* roi,
+                        const double* illumination, double dx, double dy, double* out) {
+  long n = (long)nx * ny;
+  double* irr = (double*)malloc(sizeof(double) * n);
+  double* tgt = (double*)malloc(sizeof(double) * n);
+  for (long k = 0; k < n; k++) irr[k] = fre[k] * fre[k] + fim[k] * fim[k];
+  double cell = sdx * sdy;
+  memcpy(tgt, target_irr, sizeof(double) * n);
+  double spt = 0, stt = 0;
+  for (long k = 0; k < n; k++) spt += roi ? irr[k] * roi[k] : irr[k];
+  for (long k = 0; k < n; k++) stt += tgt[k];
+  double pt = spt * cell, tt = stt * cell;
+  double s = tt > 0 ? pt / tt : 0;
+  for (long k = 0; k < n; k++) tgt[k] *= s;
+  double sinc = 0;
+  for (long k = 0; k < n; k++) sinc += illumination[k];
+  double incident = sinc * dx * dy;
+  double stot = 0;
+  for (long k = 0; k < n; k++) stot += irr[k];
+  double total = stot * cell;
+  double inSignal = spt * cell;
+  double num = 0, den = 0;
+  for (long k = 0; k < n; k++) {
+    double m = roi ? roi[k] : 1;
+    if (m <= 0) continue;
+    double d = irr[k] - tgt[k];
+    num += d * d;
+    den += tgt[k] * tgt[k];
+  }
+  out[0] = den > 0 ? sqrt(num / den) : 0;
+  out[1] = incident > 0 ? inSignal / incident : 0;
+  out[2] = total > 0 ? inSignal / total : 0;
+  out[3] = inSignal;
+  out[4] = total;
+  out[5] = incident;
+  free(irr);
+  free(tgt);
+}
+
+/* src/doe.js:817-829: targetAmp = sqrt(max(0, irr)), then scaled so that
+ * sum(targetAmp^2) equals sum(illumination^2), both summed sequentially. */
+void orc_prepare_target(const double* irr, const double* illumination, long n, double* out) {
+  for (long k = 0; k < n; k++) out[k] = sqrt(fmax(0, irr[k]));
+  double inPower = 0;
+  for (long k = 0; k < n; k++) inPower += illumination[k] * illumination[k];
+  double tPower = 0;
+  for (long k = 0; k < n; k++) tPower += out[k] * out[k];
+  if (tPower > 0) {
+    double s = sqrt(inPower / tPower);
+    for (long k = 0; k < n; k++) out[k] *= s;
+  }
+}
