@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Benchmark of the propagate-and-retrieve engine on B200.
+
+Default workload (one "step" = one pass over the whole batch): the batched
+angular-spectrum focus sweep of 64 fields of 1024x1024 complex64 (pitch 4 um,
+wavelength per field from {450, 532, 633} nm, Gaussian beam of waist 200-800 um
+times a seeded phase screen of 20 random Zernike terms up to radial order 6 with
+rms 0-3 rad), each propagated to 64 distances drawn uniformly in 15-48 mm with
+the band-limited, raised-cosine-apodised transfer function: 4096 propagations
+per step. Inputs (512 MiB) and outputs (32 GiB) are larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). `--impl reference` times the FP64 CPU port of the
+reference's propagateAngularSpectrum (the reference is JavaScript and no JS
+runtime exists on the GPU box) on all host cores over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NX = NY = 1024
+NFIELDS, NZ = 64, 64
+DX = 4e-6
+LAMBDAS = (450e-9, 532e-9, 633e-9)
+BYTES_PER_PX = 16  # read complex64 spectrum + write complex64 output, per output plane
+METRIC = "1024^2 ASM props/s (batched band-limited focus sweep)"
+CONFIG = {"workload": "asm_focus_sweep", "fields": NFIELDS, "distances_per_field": NZ, "grid": [NX, NY],
+          "pitch_um": DX * 1e6, "lambda_nm": [450, 532, 633], "z_mm": [15, 48], "band_limit": True,
+          "soft_edge": 0.02, "l2_flush": "inputs 512 MiB and outputs 32 GiB exceed L2"}
+
+
+def xorshift_stream(seed):
+    """makeRng (reference src/doe.js:65-75) as a Python generator of [0, 1) doubles."""
+    s = (int(seed) & 0xFFFFFFFF) or 1
+    while True:
+        s ^= (s << 13) & 0xFFFFFFFF
+        s ^= s >> 17
+        s ^= (s << 5) & 0xFFFFFFFF
+        yield s / 4294967296.0
+
+
+def zernike_terms(nmax=6):
+    return [(n, m) for n in range(1, nmax + 1) for m in range(-n, n + 1, 2)]
+
+
+def workload_params(seed=2024):
+    """Per-field wavelength, waist, rms, Zernike terms/coefficients and distances."""
+    rng = xorshift_stream(seed)
+    terms = zernike_terms()
+    fields = []
+    for f in range(NFIELDS):
+        lam = LAMBDAS[int(next(rng) * 3) % 3]
+        waist = 200e-6 + 600e-6 * next(rng)
+        rms = 3.0 * next(rng)
+        order = sorted(range(len(terms)), key=lambda k: next(rng))[:20]
+        coef = [(terms[k], 2 * next(rng) - 1) for k in order]
+        z = [15e-3 + 33e-3 * next(rng) for _ in range(NZ)]
+        fields.append({"lam": lam, "waist": waist, "rms": rms, "coef": coef, "z": z})
+    return fields
+
+
+def synth_fields(params, device):
+    """Complex64 fields on the device: Gaussian amplitude x exp(i * Zernike screen)."""
+    import torch
+    n = NX
+    i = torch.arange(n, device=device, dtype=torch.float64)
+    u = (i - n / 2) / (n / 2)
+    V, U = torch.meshgrid(u, u, indexing="ij")
+    r = torch.hypot(U, V)
+    th = torch.atan2(V, U)
+    disc = r <= 1
+    x = (i - n / 2) * DX
+    Y, X = torch.meshgrid(x, x, indexing="ij")
+    r2 = X * X + Y * Y
+    basis = {}
+    for (nn, m) in zernike_terms():
+        am = abs(m)
+        rad = torch.zeros_like(r)
+        for s in range((nn - am) // 2 + 1):
+            c = ((-1) ** s) * math.factorial(nn - s) / (
+                math.factorial(s) * math.factorial((nn + am) // 2 - s) * math.factorial((nn - am) // 2 - s))
+            rad = rad + c * r ** (nn - 2 * s)
+        ang = torch.cos(m * th) if m >= 0 else torch.sin(-m * th)
+        basis[(nn, m)] = torch.where(disc, rad * ang, torch.zeros_like(r))
+    out = torch.empty((len(params), n, n), dtype=torch.complex64, device=device)
+    for f, p in enumerate(params):
+        ph = torch.zeros_like(r)
+        for (t, a) in p["coef"]:
+            ph = ph + a * basis[t]
+        cur = torch.sqrt(torch.mean(ph[disc] ** 2))
+        ph = ph * (p["rms"] / cur if cur > 0 else 0.0)
+        amp = torch.exp(-r2 / (p["waist"] ** 2))
+        out[f] = torch.polar(amp, ph).to(torch.complex64)
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_read(E, ctx):
+    names = C.create_string_buffer(64 * 64)
+    ms = (C.c_double * 64)()
+    cnt = (C.c_ulonglong * 64)()
+    L = ctx.lib
+    L.doe_ctx_profile_read.restype = C.c_int
+    L.doe_ctx_profile_read.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_ulonglong)]
+    n = L.doe_ctx_profile_read(ctx.h, 64, names, 64, ms, cnt)
+    out = {}
+    for k in range(max(n, 0)):
+        nm = names.raw[k * 64:(k + 1) * 64].split(b"\0")[0].decode()
+        out[nm] = (ms[k], int(cnt[k]))
+    return out
+
+
+# ----------------------------------------------------------------- CPU (oracle port)
+def cpu_sample(params, fields_np, nplanes, threads):
+    """Time `nplanes` FP64 propagations of the workload on `threads` host threads."""
+    from oracle import oracle as O
+    O.build()
+    jobs = []
+    nf = len(fields_np)
+    for k in range(nplanes):
+        f = k % nf
+        jobs.append((f, params[f]["lam"], params[f]["z"][(k // nf) % NZ]))
+    planes = {}
+    for f, _, _ in jobs:
+        if f not in planes:
+            a = fields_np[f].astype(np.complex128).ravel()
+            planes[f] = (np.ascontiguousarray(a.real), np.ascontiguousarray(a.imag))
+    idx = [0]
+    lock = threading.Lock()
+
+    def worker():
+        while True:
+            with lock:
+                if idx[0] >= len(jobs):
+                    return
+                f, lam, z = jobs[idx[0]]
+                idx[0] += 1
+            re, im = planes[f]
+            O.asm(re, im, NX, NY, DX, DX, lam, z, True, True, 0.02)  # ctypes releases the GIL
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    return time.perf_counter() - t0
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    params = workload_params()
+    # same field construction as the GPU arm (fields 0-3), evaluated on the host
+    fields_np = synth_fields(params[:4], "cpu").numpy()
+    threads = os.cpu_count() or 1
+    per_step = threads
+    for _ in range(args.warmup):
+        cpu_sample(params, fields_np, min(per_step, 2), threads)
+    times = [cpu_sample(params, fields_np, per_step, threads) for _ in range(args.steps)]
+    t = sum(times)
+    value = per_step * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": CONFIG,
+            "cpu_baseline": {"value": value, "unit": "props/s", "cores": threads, "kind": "port",
+                             "sample": f"{per_step} planes of the workload per step (fields 0-3), one plane per "
+                                       f"thread, FP64 restatement of propagateAngularSpectrum; the reference "
+                                       f"is JavaScript and no JS runtime exists on this machine"},
+            "e2e": {"value": value, "unit": "props/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-fields", type=int, default=4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--fields", type=int, default=NFIELDS,
+                    help="fields per step (profiling runs use fewer; the benchmark uses 64)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+
+    import diffractiveopticalelement_b200 as E
+    ctx = E.Context(local)
+    L = ctx.lib
+    L.doe_ctx_launch_count.restype = C.c_ulonglong
+    L.doe_ctx_launch_count.argtypes = [C.c_void_p]
+    L.doe_ctx_set_profiling.argtypes = [C.c_void_p, C.c_int]
+
+    params = workload_params(seed=2024 + rank)[:max(1, min(args.fields, NFIELDS))]
+    nfields = len(params)
+    fields = synth_fields(params, device)
+    out = torch.empty((nfields * NZ, NY, NX), dtype=torch.complex64, device=device)
+    lam = np.array([p["lam"] for p in params], dtype=np.float64)
+    zs = np.array([z for p in params for z in p["z"]], dtype=np.float64)
+    dp = C.POINTER(C.c_double)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+
+    def step():
+        ctx.check(L.doe_asm_sweep_dev(ctx.h, fields.data_ptr(), nfields, NX, NY, DX, DX, lam.ctypes.data_as(dp),
+                                      zs.ctypes.data_as(dp), NZ, 1, 1, 0.02, out.data_ptr()))
+
+    # shape autotuning for this grid and geometry (untimed set-up)
+    L.doe_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                               C.POINTER(C.c_int)]
+    chosen = (C.c_int * 5)()
+    ctx.check(L.doe_autotune(ctx.h, NX, NY, DX, DX, 532e-9, 0.03, chosen))
+    tuned = {"fft_row": chosen[0], "fft_col": chosen[1], "sweep_row": chosen[2], "sweep_col": chosen[3],
+             "sweep_group": chosen[4]}
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+
+    # ---- timed region
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = L.doe_ctx_launch_count(ctx.h)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = int(L.doe_ctx_launch_count(ctx.h) - n0)
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    props = nfields * NZ * args.steps * world
+    value = props / (ms / 1000.0)
+
+    # ---- per-kernel durations (instrumented step right after the timed region)
+    L.doe_ctx_set_profiling(ctx.h, 1)
+    step()
+    prof = profile_read(E, ctx)
+    L.doe_ctx_set_profiling(ctx.h, 0)
+    peak, peak_kind = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else None
+    roofline = None
+    if dom:
+        name, (tot_ms, cnt) = dom
+        # column pass: read spectrum + write intermediate; row pass: read intermediate + write output
+        planes_per_launch = nfields * NZ / cnt
+        bytes_per_launch = planes_per_launch * NX * NY * 16
+        avg_s = tot_ms / cnt / 1000.0
+        achieved = bytes_per_launch / avg_s / 1e9
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                    "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6,
+                    "launches": cnt,
+                    "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()}}
+        sweep_bytes = nfields * NZ * NX * NY * BYTES_PER_PX
+        roofline["sweep_frac"] = (sweep_bytes / (ms / 1000.0 / args.steps) / 1e9) / peak
+
+    # ---- e2e through the reference-facing host-buffer call (focusSweep, FP64 planes)
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        nf = max(1, min(args.e2e_fields, nfields))
+        n = NX * NY
+        hin = C.c_void_p()
+        hout = C.c_void_p()
+        ctx.check(L.doe_host_alloc(ctx.h, C.byref(hin), 2 * n * 8 * nf))
+        ctx.check(L.doe_host_alloc(ctx.h, C.byref(hout), 2 * n * NZ * 8))
+        hin_a = np.ctypeslib.as_array((C.c_double * (2 * n * nf)).from_address(hin.value))
+        hout_a = np.ctypeslib.as_array((C.c_double * (2 * n * NZ)).from_address(hout.value))
+        src = fields[:nf].cpu().numpy().astype(np.complex128).reshape(nf, -1)
+        for f in range(nf):
+            hin_a[2 * n * f:2 * n * f + n] = src[f].real
+            hin_a[2 * n * f + n:2 * n * (f + 1)] = src[f].imag
+        reps = max(1, min(args.steps, 3))
+
+        def e2e_step():
+            for f in range(nf):
+                base = hin.value + 2 * n * 8 * f
+                ctx.check(L.doe_asm_sweep(ctx.h, C.cast(base, dp), C.cast(base + n * 8, dp), NX, NY, DX, DX,
+                                          float(lam[f]), zs[f * NZ:(f + 1) * NZ].ctypes.data_as(dp), NZ, 1, 1,
+                                          0.02, C.cast(hout.value, dp), C.cast(hout.value + n * NZ * 8, dp)))
+        e2e_step()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            e2e_step()
+        dt = (time.perf_counter() - t0) / reps
+        e2e = {"value": nf * NZ / dt, "unit": "props/s", "h2d_bytes_per_step": nf * 2 * n * 8,
+               "d2h_bytes_per_step": nf * NZ * 2 * n * 8,
+               "sample": f"{nf} fields x {NZ} distances per step through doe_asm_sweep "
+                         f"(FP64 split planes in pinned host memory, copies inside the timed region)"}
+        _ = hout_a
+        L.doe_host_free(ctx.h, hin)
+        L.doe_host_free(ctx.h, hout)
+
+    # ---- CPU baseline (oracle port on this box's host cores)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        host_fields = fields[:4].cpu().numpy()
+        nplanes = threads * 2
+        t = cpu_sample(params, host_fields, nplanes, threads)
+        cpu = {"value": nplanes / t, "unit": "props/s", "cores": threads, "kind": "port",
+               "sample": f"{nplanes} band-limited 1024^2 propagations of the workload (fields 0-3) on {threads} "
+                         f"threads, FP64 C restatement of propagateAngularSpectrum (no JS runtime on this box)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32), fp64 phase reduction",
+                "data": "synthetic", "config": dict(CONFIG, fields=nfields, tuned_variants=tuned), "clocks": clocks, "roofline": roofline,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    del out, fields
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -7,12 +7,15 @@
 // Here the phase in cycles is split exactly as
 //   z sqrt(1/l^2 - f^2) = Z - (Z/2) u - Z u^2 / (2 (1 + sqrt(1-u))^2),
 //   Z = z / lambda,  u = lambda^2 (fx^2 + fy^2) = ux + uy,
-// where frac(Z) and frac((Z/2) u_axis) are reduced mod 1 in FP64 per plane / per
-// axis bin (tables below) and only the small last term is evaluated in FP32 per
-// pixel. Pixels whose last term would exceed 2 cycles (u > ucut), including every
-// pixel near the evanescent boundary, take an FP64 path that mirrors the
-// reference's `invL2 - fx*fx - fy*fy` test exactly. The reduced cycle count goes
-// through FP32 sincospif.
+// The first two terms are separable: per axis bin the table holds the unit
+// complex factor exp(i 2 pi (frac(Z) - frac((Z/2) u_x))) (x bins) or
+// exp(-i 2 pi frac((Z/2) u_y)) (y bins), reduced and evaluated in FP64 once per
+// plane. Per pixel only the small last term q (|q| <= 2 cycles) is evaluated in
+// FP32 and reduced to [-1/2, 1/2] cycles, so its sincos argument stays in
+// [-pi, pi] where the SFU sin/cos error is below 4e-7; H is the product of the
+// three factors and the band-limit window. Pixels with q above 2 cycles (u > ucut),
+// which includes every pixel near the evanescent boundary, take an FP64 path that
+// mirrors the reference's `invL2 - fx*fx - fy*fy` test exactly.
 #pragma once
 #include "engine.cuh"
 
@@ -30,9 +33,10 @@ struct AsmPlane {
   int evanescent; // 1: zero the evanescent band (reference default)
 };
 
-// Per-bin axis entry: u = (lambda f)^2, p = frac((Z/2) u), w = band-limit window.
-struct AxisBin {
-  float u, p, w, pad;
+// Per-bin axis entry: separable unit phase factor (er, ei), u = (lambda f)^2 and
+// the band-limit window w.
+struct __align__(16) AxisBin {
+  float er, ei, u, w;
 };
 
 struct AsmGroupArgs {
@@ -70,7 +74,7 @@ __device__ __forceinline__ double d_local_frequency_limit(int n, double d, doubl
 }
 
 // One thread per (plane, axis bin); thread 0 of each plane also fills AsmPlane.
-__global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
+static __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
   const int p = blockIdx.y;
   const double lam = a.lam[p], z = a.z[p];
   const int total = a.nx + a.ny;
@@ -86,7 +90,13 @@ __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
     const double u = lam * lam * f2;
     AxisBin b;
     b.u = (float)u;
-    b.p = (float)d_frac(0.5 * (z / lam) * u);
+    // x bins carry frac(Z) - frac((Z/2) u_x), y bins -frac((Z/2) u_y) (cycles)
+    const double Z = z / lam;
+    const double cyc = isx ? d_frac(d_frac(Z) - d_frac(0.5 * Z * u)) : -d_frac(0.5 * Z * u);
+    double sn, cs;
+    sincospi(2.0 * cyc, &sn, &cs);
+    b.er = (float)cs;
+    b.ei = (float)sn;
     double w = 1.0;
     if (a.band_limit) {
       const double lim0 = d_local_frequency_limit(n, d, lam, z);
@@ -95,7 +105,6 @@ __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
       w = d_soft_window(fabs(f), lim, lim * (1.0 - a.soft_edge));
     }
     b.w = (float)w;
-    b.pad = 0.f;
     if (isx) {
       t.xt[(long)p * a.nx + k] = b;
       if (p == 0) t.xf2[k] = f2;
@@ -129,35 +138,70 @@ __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
   }
 }
 
-// Transfer function at unshifted FFT bin (kx, ky) of plane p.
-__device__ __forceinline__ float2 asm_h(const AsmTables& t, int nx, int ny, int p, int kx, int ky) {
-  const AxisBin bx = t.xt[(long)p * nx + kx];
-  const AxisBin by = t.yt[(long)p * ny + ky];
-  const float w = bx.w * by.w;
-  const AsmPlane& P = t.pl[p];
-  const float u = bx.u + by.u;
-  float c;
-  if (u <= P.ucut) {
-    const float s = 1.f + sqrtf(1.f - u);
-    const float q = P.hz * (u * u) / (s * s);
-    c = P.c0 - bx.p - by.p - q;
+// FP64 evaluation for pixels beyond the FP32 fast-path range (u > ucut):
+// exact reference classification (src/propagate.js:80-98) and FP64 phase.
+static __device__ __noinline__ float2 asm_h_slow(const AsmPlane* __restrict__ pl, const double* __restrict__ xf2,
+                                          const double* __restrict__ yf2, int ky, float w) {
+  const AsmPlane& P = *pl;
+  const double arg = (P.invL2 - *xf2) - yf2[ky];
+  double cyc;
+  if (arg >= 0.0) {
+    cyc = P.z * sqrt(arg);
+  } else if (P.evanescent) {
+    return make_float2(0.f, 0.f);
   } else {
-    // exact reference classification and FP64 phase (src/propagate.js:80-98)
-    const double arg = (P.invL2 - t.xf2[kx]) - t.yf2[ky];
-    double cyc;
-    if (arg >= 0.0) {
-      cyc = P.z * sqrt(arg);
-    } else if (P.evanescent) {
-      return make_float2(0.f, 0.f);
-    } else {
-      cyc = P.z * sqrt(-arg);
-    }
-    c = (float)d_frac(cyc);
+    cyc = P.z * sqrt(-arg);
   }
+  float c = (float)d_frac(cyc);
   c -= rintf(c);
   float sn, cs;
   sincospif(2.f * c, &sn, &cs);
   return make_float2(w * cs, w * sn);
+}
+
+// Invariants of one column (fixed bin kx) of plane p, loaded once per thread.
+struct AsmCol {
+  float er, ei, u, w;   // x-bin factor, u_x, window
+  const AxisBin* yt;    // y-bins of plane p
+  float hz, ucut;
+  int p, kx;
+};
+
+__device__ __forceinline__ AsmCol asm_col(const AsmTables& t, int nx, int ny, int p, int kx) {
+  const AxisBin bx = t.xt[(long)p * nx + kx];
+  AsmCol c;
+  c.er = bx.er;
+  c.ei = bx.ei;
+  c.u = bx.u;
+  c.w = bx.w;
+  c.yt = t.yt + (long)p * ny;
+  c.hz = t.pl[p].hz;
+  c.ucut = t.pl[p].ucut;
+  c.p = p;
+  c.kx = kx;
+  return c;
+}
+
+// Transfer function at bin (c.kx, ky).
+__device__ __forceinline__ float2 asm_h_col(const AsmCol& c, const AsmTables& t, int ky) {
+  const AxisBin by = c.yt[ky];
+  const float w = c.w * by.w;
+  const float u = c.u + by.u;
+  const float om = fmaxf(1.f - u, 1e-3f);
+  const float s = 1.f + om * rsqrtf(om);          // 1 + sqrt(1 - u)
+  float q = __fdividef(c.hz * (u * u), s * s);      // Z u^2 / (2 (1 + sqrt(1-u))^2)
+  q -= rintf(q);
+  float sn, cs;
+  __sincosf(-6.283185307179586f * q, &sn, &cs);     // |arg| <= pi
+  const float2 e = cmul(cmul(make_float2(c.er, c.ei), make_float2(by.er, by.ei)), make_float2(cs, sn));
+  float2 h = make_float2(w * e.x, w * e.y);
+  if (u > c.ucut && w != 0.f) h = asm_h_slow(t.pl + c.p, t.xf2 + c.kx, t.yf2, ky, w);
+  return h;
+}
+
+// Transfer function at unshifted FFT bin (kx, ky) of plane p.
+__device__ __forceinline__ float2 asm_h(const AsmTables& t, int nx, int ny, int p, int kx, int ky) {
+  return asm_h_col(asm_col(t, nx, ny, p, kx), t, ky);
 }
 
 inline int asm_tables_bytes(int nplanes, int nx, int ny, size_t* bytes) {
@@ -194,6 +238,7 @@ inline int asm_build_tables(doe_ctx* c, const AsmGroupArgs& a, AsmTables* out, i
   *out = asm_tables_carve(base, a.nplanes, a.nx, a.ny);
   const int total = a.nx + a.ny;
   dim3 grid((total + 255) / 256, a.nplanes);
+  LaunchScope ls(c, "asm_tables");
   asm_tables_kernel<<<grid, 256, 0, c->stream>>>(a, *out);
   DOE_CUDA(c, cudaGetLastError());
   return DOE_OK;

@@ -20,7 +20,8 @@ extern "C" int doe_ctx_create(int device, doe_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return DOE_ERR_CUDA;
   doe_ctx* c = new doe_ctx();
   c->device = device;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return DOE_ERR_CUDA;
   }
@@ -51,6 +52,16 @@ extern "C" void doe_ctx_destroy(doe_ctx* c) {
   for (int s = 0; s < kSlotCount; ++s)
     if (c->slot[s]) cudaFree(c->slot[s]);
   if (c->tw) cudaFree(c->tw);
+  for (auto& r : c->prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  for (auto e : c->sync_ev) cudaEventDestroy(e);
+  if (c->aux) {
+    cudaStreamSynchronize(c->aux);
+    cudaStreamDestroy(c->aux);
+  }
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -64,6 +75,72 @@ extern "C" int doe_ctx_synchronize(doe_ctx* c) {
   if (!c) return DOE_ERR_BAD_ARG;
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
+}
+
+extern "C" unsigned long long doe_ctx_launch_count(doe_ctx* c) { return c ? c->launches : 0ull; }
+
+extern "C" int doe_ctx_set_profiling(doe_ctx* c, int on) {
+  if (!c) return DOE_ERR_BAD_ARG;
+  c->prof_on = on ? 1 : 0;
+  return DOE_OK;
+}
+
+// Fold pending launch events into per-label totals (synchronises the stream).
+extern "C" int doe_ctx_profile_read(doe_ctx* c, int max_entries, char* names, int name_len, double* total_ms,
+                                    unsigned long long* count) {
+  if (!c) return DOE_ERR_BAD_ARG;
+  DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::vector<std::string> labels;
+  std::vector<double> ms;
+  std::vector<unsigned long long> cnt;
+  for (auto& r : c->prof) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    size_t k = 0;
+    while (k < labels.size() && labels[k] != r.name) ++k;
+    if (k == labels.size()) {
+      labels.push_back(r.name);
+      ms.push_back(0.0);
+      cnt.push_back(0);
+    }
+    ms[k] += t;
+    cnt[k] += 1;
+    c->ev_pool.push_back(r.a);
+    c->ev_pool.push_back(r.b);
+  }
+  c->prof.clear();
+  const int n = (int)labels.size() < max_entries ? (int)labels.size() : max_entries;
+  for (int k = 0; k < n; ++k) {
+    if (names && name_len > 0) {
+      snprintf(names + (size_t)k * name_len, name_len, "%s", labels[k].c_str());
+    }
+    if (total_ms) total_ms[k] = ms[k];
+    if (count) count[k] = cnt[k];
+  }
+  return n;
+}
+
+extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) {
+  if (!c || !key) return DOE_ERR_BAD_ARG;
+  const std::string k(key);
+  if (k == "sweep_group") {
+    if (value < 0 || value > 64) return set_err(c, DOE_ERR_BAD_ARG, "sweep_group must be in [0, 64]");
+    c->tune_sweep_group = (long)value;
+    return DOE_OK;
+  }
+  // "<kind>_row" / "<kind>_col" with value = (log2(n) << 8) | variant
+  const char* kinds[] = {"fft", "sweep", "design"};
+  for (int kind = 0; kind < 3; ++kind) {
+    for (int rc = 0; rc < 2; ++rc) {
+      if (k == std::string(kinds[kind]) + (rc ? "_col" : "_row")) {
+        const int lg = (int)((value >> 8) & 0xff), var = (int)(value & 0xff);
+        if (lg > kMaxLog2) return set_err(c, DOE_ERR_BAD_ARG, "tuning: log2 length %d out of range", lg);
+        (rc ? c->tune_col : c->tune_row)[kind][lg] = (unsigned char)var;
+        return DOE_OK;
+      }
+    }
+  }
+  return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
 }
 
 extern "C" int doe_host_alloc(doe_ctx* c, void** ptr, unsigned long long bytes) {

@@ -34,10 +34,24 @@ enum Slot {
 
 }  // namespace doe
 
+struct doe_prof_rec {
+  const char* name;
+  cudaEvent_t a, b;
+};
+
 struct doe_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;          // second stream for pipelined passes
+  std::vector<cudaEvent_t> sync_ev;    // events ordering the two streams
+  long tune_sweep_group = 0;           // planes per sweep launch pair (0 = from L2 size)
+  unsigned char tune_row[4][16] = {};  // chosen row-shape variant per [kind][log2 N]
+  unsigned char tune_col[4][16] = {};  // chosen column-shape variant per [kind][log2 N]
   std::string err;
+  unsigned long long launches = 0;     // kernels launched by this context
+  int prof_on = 0;                     // time every launch with CUDA events
+  std::vector<doe_prof_rec> prof;      // pending event pairs
+  std::vector<cudaEvent_t> ev_pool;    // recycled events
   float2* tw = nullptr;  // twiddle tables: table for length N starts at tw + N
   void* slot[doe::kSlotCount] = {};
   size_t slot_bytes[doe::kSlotCount] = {};
@@ -137,59 +151,147 @@ inline int with_n(int n, F&& f) {
   }
 }
 
-template <int N, class Op>
-inline int launch_row(doe_ctx* c, const Op& op, int nplanes, int nlines) {
-  using Cfg = RowCfg<N>;
-  auto kern = row_kernel<N, Op>;
-  static bool attr_set = false;
-  if (!attr_set && Cfg::SMEM > 48 * 1024) {
-    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
-    attr_set = true;
+// Kernel label used by the launch profiler: Op::kName when present.
+template <class Op, class = void>
+struct OpName {
+  static const char* get() { return "kernel"; }
+};
+template <class Op>
+struct OpName<Op, std::void_t<decltype(Op::kName)>> {
+  static const char* get() { return Op::kName; }
+};
+
+inline cudaEvent_t prof_event(doe_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
   }
-  const long bpp = (nlines + Cfg::V - 1) / Cfg::V;
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Bracket a launch with events when profiling is on; count every launch.
+struct LaunchScope {
+  doe_ctx* c;
+  const char* name;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  LaunchScope(doe_ctx* c_, const char* n, cudaStream_t s = nullptr) : c(c_), name(n), st(s ? s : c_->stream) {
+    ++c->launches;
+    if (c->prof_on) {
+      a = prof_event(c);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~LaunchScope() {
+    if (a) {
+      cudaEvent_t b = prof_event(c);
+      cudaEventRecord(b, st);
+      c->prof.push_back({name, a, b});
+    }
+  }
+};
+
+// Tuning kinds: each family of fused operators keeps its own shape choice.
+enum TuneKind { kTuneFft = 0, kTuneSweep = 1, kTuneDesign = 2, kTuneKinds = 4 };
+
+inline int ilog2i(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+template <class S, class Op>
+inline int launch_row(doe_ctx* c, const Op& op, int nplanes, int nlines, cudaStream_t stream = nullptr) {
+  auto kern = row_kernel<S, Op>;
+  static unsigned long long attr_set = 0;  // one bit per device
+  if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
+    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+    attr_set |= 1ull << (c->device & 63);
+  }
+  const long bpp = (nlines + S::V - 1) / S::V;
   const long grid = bpp * (long)nplanes;
   if (grid <= 0) return DOE_OK;
   if (grid > 0x7fffffffL) return set_err(c, DOE_ERR_UNSUPPORTED, "row pass grid too large");
-  kern<<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM, c->stream>>>(op, c->tw + N, nlines);
+  cudaStream_t st = stream ? stream : c->stream;
+  LaunchScope ls(c, OpName<Op>::get(), st);
+  kern<<<(unsigned)grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, nlines);
   DOE_CUDA(c, cudaGetLastError());
   return DOE_OK;
 }
 
-template <int N, class Op>
-inline int launch_col(doe_ctx* c, const Op& op, int nplanes, int ncols) {
-  using Cfg = ColCfg<N>;
-  auto kern = col_kernel<N, Op>;
-  static bool attr_set = false;
-  if (!attr_set && Cfg::SMEM > 48 * 1024) {
-    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
-    attr_set = true;
+template <class S, class Op>
+inline int launch_col(doe_ctx* c, const Op& op, int nplanes, int ncols, cudaStream_t stream = nullptr) {
+  auto kern = col_kernel<S, Op>;
+  static unsigned long long attr_set = 0;  // one bit per device
+  if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
+    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+    attr_set |= 1ull << (c->device & 63);
   }
   if (nplanes <= 0) return DOE_OK;
   if (nplanes > 65535) return set_err(c, DOE_ERR_UNSUPPORTED, "column pass: at most 65535 planes per launch");
-  dim3 grid((ncols + Cfg::C - 1) / Cfg::C, nplanes);
-  kern<<<grid, Cfg::THREADS, Cfg::SMEM, c->stream>>>(op, c->tw + N, ncols);
+  dim3 grid((ncols + S::C - 1) / S::C, nplanes);
+  cudaStream_t st = stream ? stream : c->stream;
+  LaunchScope ls(c, OpName<Op>::get(), st);
+  kern<<<grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, ncols);
   DOE_CUDA(c, cudaGetLastError());
   return DOE_OK;
 }
 
-// Blocks per plane of each pass (needed to size reduction partials).
-template <int N>
-inline int row_blocks_per_plane(int nlines) {
-  return (nlines + RowCfg<N>::V - 1) / RowCfg<N>::V;
+// Pick element I of a shape list by runtime index (index 0 when out of range).
+template <class L, int I = 0, class F>
+inline int select_shape(int idx, F& f) {
+  if constexpr (I < (int)std::tuple_size<L>::value) {
+    if (idx == I) return f(std::tuple_element_t<I, L>{});
+    return select_shape<L, I + 1>(idx, f);
+  } else {
+    return f(std::tuple_element_t<0, L>{});
+  }
 }
-template <int N>
-inline int col_blocks_per_plane(int ncols) {
-  return (ncols + ColCfg<N>::C - 1) / ColCfg<N>::C;
+
+// f(Shape{}) with the row shape the context selected for length n and `kind`.
+template <class F>
+inline int with_row(doe_ctx* c, int n, int kind, F&& f) {
+  return with_n(n, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    return select_shape<typename RowVariants<N>::list>(c->tune_row[kind][ilog2i(N)], f);
+  });
 }
-inline int row_bpp(int n, int nlines) {
-  int r = 0;
-  with_n(n, [&](auto NC) { r = row_blocks_per_plane<decltype(NC)::value>(nlines); return 0; });
-  return r;
+template <class F>
+inline int with_col(doe_ctx* c, int n, int kind, F&& f) {
+  return with_n(n, [&](auto NC) {
+    constexpr int N = decltype(NC)::value;
+    return select_shape<typename ColVariants<N>::list>(c->tune_col[kind][ilog2i(N)], f);
+  });
 }
-inline int col_bpp(int n, int ncols) {
-  int r = 0;
-  with_n(n, [&](auto NC) { r = col_blocks_per_plane<decltype(NC)::value>(ncols); return 0; });
-  return r;
+// Default shapes only (operators that are not tuned).
+template <class F>
+inline int with_row0(int n, F&& f) {
+  return with_n(n, [&](auto NC) { return f(typename DefRow<decltype(NC)::value>::type{}); });
+}
+template <class F>
+inline int with_col0(int n, F&& f) {
+  return with_n(n, [&](auto NC) { return f(typename DefCol<decltype(NC)::value>::type{}); });
+}
+
+// Number of variants for length n (for the autotuner).
+inline int row_variant_count(int n) {
+  return with_n(n, [&](auto NC) { return (int)std::tuple_size<typename RowVariants<decltype(NC)::value>::list>::value; });
+}
+inline int col_variant_count(int n) {
+  return with_n(n, [&](auto NC) { return (int)std::tuple_size<typename ColVariants<decltype(NC)::value>::list>::value; });
+}
+
+// Event k of the context's ordering pool (grown on demand).
+inline cudaEvent_t sync_event(doe_ctx* c, size_t k) {
+  while (c->sync_ev.size() <= k) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    c->sync_ev.push_back(e);
+  }
+  return c->sync_ev[k];
 }
 
 // Centred index of FFT bin k (fftshift position) and its signed frequency index,

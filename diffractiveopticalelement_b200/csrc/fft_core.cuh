@@ -155,57 +155,48 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[RA]) {
 }
 
 // ---------------------------------------------------------------- plans
-// Radix sequence per length. RMAX registers per thread, T = N / RMAX threads per
-// vector; in pass p each thread runs RMAX / R_p butterflies. Symmetric plans
-// (first radix == last radix) let two transforms chain in registers.
-template <int N>
-struct Plan;
-#define DOE_PLAN(NN, NP_, R0, R1, R2)                           \
-  template <>                                                   \
-  struct Plan<NN> {                                             \
-    static constexpr int NP = NP_;                              \
-    static constexpr int r0 = R0, r1 = R1, r2 = R2;             \
-    static constexpr int RMAX = (R0 > R1 ? (R0 > R2 ? R0 : R2) : (R1 > R2 ? R1 : R2)); \
-    static constexpr int T = NN / RMAX;                         \
-    static constexpr __host__ __device__ int radix(int p) { return p == 0 ? R0 : (p == 1 ? R1 : R2); } \
-  };
-DOE_PLAN(1, 1, 1, 1, 1)
-DOE_PLAN(2, 1, 2, 1, 1)
-DOE_PLAN(4, 1, 4, 1, 1)
-DOE_PLAN(8, 1, 8, 1, 1)
-DOE_PLAN(16, 1, 16, 1, 1)
-DOE_PLAN(32, 1, 32, 1, 1)
-DOE_PLAN(64, 2, 8, 8, 1)
-DOE_PLAN(128, 2, 16, 8, 1)
-DOE_PLAN(256, 2, 16, 16, 1)
-DOE_PLAN(512, 3, 8, 8, 8)
-DOE_PLAN(1024, 2, 32, 32, 1)
-DOE_PLAN(2048, 3, 16, 8, 16)
-DOE_PLAN(4096, 3, 16, 16, 16)
-DOE_PLAN(8192, 3, 32, 8, 32)
-#undef DOE_PLAN
-
-template <int N>
-constexpr int plan_radix(int p) {
-  return Plan<N>::radix(p);
-}
-template <int N, int P>
-struct PassNs {  // product of the radices before pass P
-  static constexpr int value = PassNs<N, P - 1>::value * Plan<N>::radix(P - 1);
+// A plan is a radix sequence for one length. RMAX registers per thread,
+// T = N / RMAX threads per vector; in pass p each thread runs RMAX / R_p
+// butterflies. Symmetric plans (first radix == last radix) let two transforms
+// chain in registers without a shared-memory re-layout.
+template <int N_, int NP_, int R0, int R1 = 1, int R2 = 1>
+struct FftPlan {
+  static constexpr int N = N_;
+  static constexpr int NP = NP_;
+  static constexpr int RMAX = (R0 > R1 ? (R0 > R2 ? R0 : R2) : (R1 > R2 ? R1 : R2));
+  static constexpr int T = N_ / RMAX;
+  static constexpr __host__ __device__ int radix(int p) { return p == 0 ? R0 : (p == 1 ? R1 : R2); }
+  static constexpr int last() { return radix(NP_ - 1); }
+  static constexpr bool symmetric() { return R0 == radix(NP_ - 1); }
+  static_assert(NP_ == 1 ? R0 == N_ : (NP_ == 2 ? R0 * R1 == N_ : R0 * R1 * R2 == N_), "radices must multiply to N");
 };
+
+// Default plan per length.
 template <int N>
-struct PassNs<N, 0> {
+struct DefaultPlan;
+template <> struct DefaultPlan<1> { using type = FftPlan<1, 1, 1>; };
+template <> struct DefaultPlan<2> { using type = FftPlan<2, 1, 2>; };
+template <> struct DefaultPlan<4> { using type = FftPlan<4, 1, 4>; };
+template <> struct DefaultPlan<8> { using type = FftPlan<8, 1, 8>; };
+template <> struct DefaultPlan<16> { using type = FftPlan<16, 1, 16>; };
+template <> struct DefaultPlan<32> { using type = FftPlan<32, 1, 32>; };
+template <> struct DefaultPlan<64> { using type = FftPlan<64, 2, 8, 8>; };
+template <> struct DefaultPlan<128> { using type = FftPlan<128, 2, 16, 8>; };
+template <> struct DefaultPlan<256> { using type = FftPlan<256, 2, 16, 16>; };
+template <> struct DefaultPlan<512> { using type = FftPlan<512, 3, 8, 8, 8>; };
+template <> struct DefaultPlan<1024> { using type = FftPlan<1024, 2, 32, 32>; };
+template <> struct DefaultPlan<2048> { using type = FftPlan<2048, 3, 16, 8, 16>; };
+template <> struct DefaultPlan<4096> { using type = FftPlan<4096, 3, 16, 16, 16>; };
+template <> struct DefaultPlan<8192> { using type = FftPlan<8192, 3, 32, 8, 32>; };
+
+template <class P, int PI>
+struct PassNs {  // product of the radices before pass PI
+  static constexpr int value = PassNs<P, PI - 1>::value * P::radix(PI - 1);
+};
+template <class P>
+struct PassNs<P, 0> {
   static constexpr int value = 1;
 };
-
-template <int N>
-constexpr int last_radix() {
-  return Plan<N>::radix(Plan<N>::NP - 1);
-}
-template <int N>
-constexpr bool plan_symmetric() {
-  return Plan<N>::radix(0) == last_radix<N>();
-}
 
 // Padded shared-memory index: one spare slot every 32 complex values keeps the
 // stride-R Stockham writes of the early passes free of bank conflicts.
@@ -226,13 +217,14 @@ struct SmemVec {
 };
 
 // ---------------------------------------------------------------- one pass
-// Apply twiddles W_{Ns R}^{r k} and the radix-R DFT for butterfly slot BI of pass P.
-template <int N, int P, bool INV, int BI>
-__device__ __forceinline__ void pass_bfly(float2 (&v)[Plan<N>::RMAX], int t, const float2* __restrict__ tw) {
-  constexpr int R = Plan<N>::radix(P);
-  constexpr int RMAX = Plan<N>::RMAX;
-  constexpr int T = Plan<N>::T;
-  constexpr int NS = PassNs<N, P>::value;
+// Apply twiddles W_{Ns R}^{r k} and the radix-R DFT for butterfly slot BI of pass PI.
+template <class P, int PI, bool INV, int BI>
+__device__ __forceinline__ void pass_bfly(float2 (&v)[P::RMAX], int t, const float2* __restrict__ tw) {
+  constexpr int N = P::N;
+  constexpr int R = P::radix(PI);
+  constexpr int RMAX = P::RMAX;
+  constexpr int T = P::T;
+  constexpr int NS = PassNs<P, PI>::value;
   if constexpr (BI < RMAX / R) {
     if constexpr (NS > 1) {
       const int j = t + BI * T;
@@ -245,87 +237,77 @@ __device__ __forceinline__ void pass_bfly(float2 (&v)[Plan<N>::RMAX], int t, con
       }
     }
     dft_reg<R, INV, BI * R>(v);
-    pass_bfly<N, P, INV, BI + 1>(v, t, tw);
+    pass_bfly<P, PI, INV, BI + 1>(v, t, tw);
   }
 }
 
-template <int N, int P, bool INV>
-__device__ __forceinline__ void pass_compute(float2 (&v)[Plan<N>::RMAX], int t, const float2* __restrict__ tw) {
-  pass_bfly<N, P, INV, 0>(v, t, tw);
-}
-
-// Write pass-P outputs to shared memory at their Stockham positions.
-template <int N, int P>
-__device__ __forceinline__ void pass_store(const float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s) {
-  constexpr int R = Plan<N>::radix(P);
-  constexpr int RMAX = Plan<N>::RMAX;
-  constexpr int T = Plan<N>::T;
-  constexpr int NS = PassNs<N, P>::value;
+// Write pass-PI outputs to shared memory at their Stockham positions.
+template <class P, int PI>
+__device__ __forceinline__ void pass_store(const float2 (&v)[P::RMAX], int t, const SmemVec& s) {
+  constexpr int R = P::radix(PI);
+  constexpr int NS = PassNs<P, PI>::value;
 #pragma unroll
-  for (int b = 0; b < RMAX / R; ++b) {
-    const int j = t + b * T;
+  for (int b = 0; b < P::RMAX / R; ++b) {
+    const int j = t + b * P::T;
     const int d = (j / NS) * NS * R + (j % NS);
 #pragma unroll
     for (int r = 0; r < R; ++r) s.at(d + r * NS) = v[b * R + r];
   }
 }
 
-// Read pass-P inputs from shared memory (element j + r N/R for butterfly j).
-template <int N, int P>
-__device__ __forceinline__ void pass_load(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s) {
-  constexpr int R = Plan<N>::radix(P);
-  constexpr int RMAX = Plan<N>::RMAX;
-  constexpr int T = Plan<N>::T;
+// Read pass-PI inputs from shared memory (element j + r N/R for butterfly j).
+template <class P, int PI>
+__device__ __forceinline__ void pass_load(float2 (&v)[P::RMAX], int t, const SmemVec& s) {
+  constexpr int R = P::radix(PI);
 #pragma unroll
-  for (int b = 0; b < RMAX / R; ++b) {
-    const int j = t + b * T;
+  for (int b = 0; b < P::RMAX / R; ++b) {
+    const int j = t + b * P::T;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[b * R + r] = s.at(j + r * (N / R));
+    for (int r = 0; r < R; ++r) v[b * R + r] = s.at(j + r * (P::N / R));
   }
 }
 
-// Element index held by register slot (b, r) before pass P (input layout).
-template <int N, int P>
+// Element index held by register slot (b, r) before pass 0 (input layout).
+template <class P>
 __device__ __forceinline__ int in_elem(int t, int slot) {
-  constexpr int R = Plan<N>::radix(P);
+  constexpr int R = P::radix(0);
   const int b = slot / R, r = slot % R;
-  return t + b * Plan<N>::T + r * (N / R);
+  return t + b * P::T + r * (P::N / R);
 }
 // Element index held by slot after the last pass (natural-order output layout).
-template <int N>
+template <class P>
 __device__ __forceinline__ int out_elem(int t, int slot) {
-  constexpr int R = last_radix<N>();
+  constexpr int R = P::last();
   const int b = slot / R, r = slot % R;
-  return t + b * Plan<N>::T + r * (N / R);
+  return t + b * P::T + r * (P::N / R);
 }
 
 // Full transform: registers hold the pass-0 input layout on entry and the
-// natural-order output layout on return. `sync` is a block or warp barrier.
-template <int N, bool INV, int P = 0, class Sync>
-__device__ __forceinline__ void fft_run(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s,
+// natural-order output layout on return. `sync` is a block barrier.
+template <class P, bool INV, int PI = 0, class Sync>
+__device__ __forceinline__ void fft_run(float2 (&v)[P::RMAX], int t, const SmemVec& s,
                                         const float2* __restrict__ tw, Sync sync) {
-  pass_compute<N, P, INV>(v, t, tw);
-  if constexpr (P + 1 < Plan<N>::NP) {
+  pass_bfly<P, PI, INV, 0>(v, t, tw);
+  if constexpr (PI + 1 < P::NP) {
     sync();  // everyone finished reading the previous contents of s
-    pass_store<N, P>(v, t, s);
+    pass_store<P, PI>(v, t, s);
     sync();
-    pass_load<N, P + 1>(v, t, s);
-    fft_run<N, INV, P + 1>(v, t, s, tw, sync);
+    pass_load<P, PI + 1>(v, t, s);
+    fft_run<P, INV, PI + 1>(v, t, s, tw, sync);
   }
 }
 
 // Re-layout registers from the output layout to the pass-0 input layout (only
 // needed for asymmetric plans when two transforms are chained).
-template <int N, class Sync>
-__device__ __forceinline__ void relayout_out_to_in(float2 (&v)[Plan<N>::RMAX], int t, const SmemVec& s, Sync sync) {
-  if constexpr (!plan_symmetric<N>()) {
-    constexpr int RMAX = Plan<N>::RMAX;
+template <class P, class Sync>
+__device__ __forceinline__ void relayout_out_to_in(float2 (&v)[P::RMAX], int t, const SmemVec& s, Sync sync) {
+  if constexpr (!P::symmetric()) {
     sync();
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) s.at(out_elem<N>(t, q)) = v[q];
+    for (int q = 0; q < P::RMAX; ++q) s.at(out_elem<P>(t, q)) = v[q];
     sync();
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) v[q] = s.at(in_elem<N, 0>(t, q));
+    for (int q = 0; q < P::RMAX; ++q) v[q] = s.at(in_elem<P>(t, q));
   }
 }
 

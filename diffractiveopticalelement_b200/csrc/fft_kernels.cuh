@@ -6,37 +6,101 @@
 // `Op` that supplies
 //   kStages            1 (one transform) or 2 (two chained transforms)
 //   kInv1, kInv2       direction of each transform
-//   load(plane, line, e)                 -> float2   input element e of the line
-//   mid(plane, line, e, float2&)                      pointwise op between stages
-//   store(plane, line, e, float2, Acc&)               consume output element e
+//   State init(plane, line)                         per-thread invariants of a line
+//   load(State&, e)                 -> float2        input element e of the line
+//   mid(State&, e, float2&)                          pointwise op between stages
+//   store(State&, e, float2, Acc&)                   consume output element e
 //   finish(plane, block_in_plane, blocks_per_plane, Acc&)   block epilogue
 // `line` is the row index y for the row kernel and the column index x for the
-// column kernel; `e` is the element position along the transformed axis.
+// column kernel; `e` is the element position along the transformed axis. init()
+// is called for inactive lines too (with a clamped line index) and must not fault.
 #pragma once
+#include <tuple>
+
 #include "fft_core.cuh"
 
 namespace doe {
 
 struct NoAcc {};
 
-// Threads per CTA and vectors per CTA chosen per transform length.
-template <int N>
-struct RowCfg {
-  static constexpr int T = Plan<N>::T;
-  static constexpr int V = (256 / T) > 0 ? (256 / T) : 1;  // vectors per CTA
+// CTA shapes. A row shape processes V vectors of a plane per CTA (one vector =
+// one row), a column shape C adjacent columns (element-major tile in shared
+// memory so a half-warp always touches one element row: conflict-free).
+template <class P, int V_>
+struct RowShape {
+  using Plan = P;
+  static constexpr int N = P::N;
+  static constexpr int V = V_;
+  static constexpr int T = P::T;
   static constexpr int THREADS = V * T;
-  static constexpr int SMEM = Plan<N>::NP > 1 ? V * padded_len<N>() * (int)sizeof(float2) : 0;
+  static constexpr int SMEM = P::NP > 1 ? V * padded_len<P::N>() * (int)sizeof(float2) : 0;
 };
 
-template <int N>
-struct ColCfg {
-  static constexpr int T = Plan<N>::T;
-  // columns per CTA: 256-512 threads, enough registers for RMAX = 32 per thread
-  static constexpr int C = Plan<N>::NP == 1 ? 128
-                           : (T >= 128 ? (512 / T > 0 ? 512 / T : 1)
-                                       : ((256 / T) < 4 ? 4 : ((256 / T) > 32 ? 32 : (256 / T))));
+template <class P, int C_>
+struct ColShape {
+  using Plan = P;
+  static constexpr int N = P::N;
+  static constexpr int C = C_;
+  static constexpr int T = P::T;
   static constexpr int THREADS = C * T;
-  static constexpr int SMEM = Plan<N>::NP > 1 ? (N * C + (N * C) / 32 + 1) * (int)sizeof(float2) : 0;
+  static constexpr int SMEM = P::NP > 1 ? (P::N * C + (P::N * C) / 32 + 1) * (int)sizeof(float2) : 0;
+};
+
+// Default shapes: ~256 threads per CTA (512 for the longest vectors).
+template <int N>
+struct DefRow {
+  using P = typename DefaultPlan<N>::type;
+  using type = RowShape<P, ((256 / P::T) > 0 ? (256 / P::T) : 1)>;
+};
+template <int N>
+struct DefCol {
+  using P = typename DefaultPlan<N>::type;
+  static constexpr int C = P::NP == 1 ? 128
+                           : (P::T >= 128 ? (512 / P::T > 0 ? 512 / P::T : 1)
+                                          : ((256 / P::T) < 4 ? 4 : ((256 / P::T) > 32 ? 32 : (256 / P::T))));
+  using type = ColShape<P, C>;
+};
+
+// Tunable shape lists (index 0 is the default). Only the large lengths, where
+// register pressure and occupancy trade against shared-memory passes, carry
+// alternatives; the autotuner measures them on the device.
+template <int N>
+struct RowVariants {
+  using list = std::tuple<typename DefRow<N>::type>;
+};
+template <int N>
+struct ColVariants {
+  using list = std::tuple<typename DefCol<N>::type>;
+};
+template <>
+struct RowVariants<1024> {
+  using list = std::tuple<RowShape<FftPlan<1024, 2, 32, 32>, 8>, RowShape<FftPlan<1024, 3, 16, 4, 16>, 4>,
+                          RowShape<FftPlan<1024, 3, 16, 4, 16>, 2>, RowShape<FftPlan<1024, 2, 32, 32>, 4>>;
+};
+template <>
+struct ColVariants<1024> {
+  using list = std::tuple<ColShape<FftPlan<1024, 2, 32, 32>, 8>, ColShape<FftPlan<1024, 3, 16, 4, 16>, 4>,
+                          ColShape<FftPlan<1024, 3, 16, 4, 16>, 8>, ColShape<FftPlan<1024, 2, 32, 32>, 4>>;
+};
+template <>
+struct RowVariants<2048> {
+  using list = std::tuple<RowShape<FftPlan<2048, 3, 16, 8, 16>, 2>, RowShape<FftPlan<2048, 3, 32, 2, 32>, 4>,
+                          RowShape<FftPlan<2048, 3, 8, 32, 8>, 1>, RowShape<FftPlan<2048, 3, 16, 8, 16>, 1>>;
+};
+template <>
+struct ColVariants<2048> {
+  using list = std::tuple<ColShape<FftPlan<2048, 3, 16, 8, 16>, 4>, ColShape<FftPlan<2048, 3, 32, 2, 32>, 4>,
+                          ColShape<FftPlan<2048, 3, 16, 8, 16>, 2>, ColShape<FftPlan<2048, 3, 32, 2, 32>, 8>>;
+};
+template <>
+struct RowVariants<512> {
+  using list = std::tuple<RowShape<FftPlan<512, 3, 8, 8, 8>, 4>, RowShape<FftPlan<512, 2, 16, 32>, 16>,
+                          RowShape<FftPlan<512, 2, 32, 16>, 16>>;
+};
+template <>
+struct ColVariants<512> {
+  using list = std::tuple<ColShape<FftPlan<512, 3, 8, 8, 8>, 4>, ColShape<FftPlan<512, 2, 16, 32>, 16>,
+                          ColShape<FftPlan<512, 2, 32, 16>, 16>>;
 };
 
 struct BlockSync {
@@ -44,12 +108,12 @@ struct BlockSync {
 };
 
 // Row pass. Grid: nplanes * ceil(nlines / V) CTAs; rows beyond nlines idle.
-template <int N, class Op>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS) row_kernel(Op op, const float2* __restrict__ tw,
-                                                                 int nlines) {
-  constexpr int T = Plan<N>::T;
-  constexpr int V = RowCfg<N>::V;
-  constexpr int RMAX = Plan<N>::RMAX;
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __restrict__ tw, int nlines) {
+  using P = typename S::Plan;
+  constexpr int T = P::T;
+  constexpr int V = S::V;
+  constexpr int RMAX = P::RMAX;
   extern __shared__ float2 smem[];
   const int lv = threadIdx.x / T;
   const int t = threadIdx.x % T;
@@ -58,34 +122,39 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS) row_kernel(Op op, const fl
   const int bip = blockIdx.x % bpp;
   const int line = bip * V + lv;
   const bool active = line < nlines;
-  SmemVec s{smem + lv * padded_len<N>(), 1, 0};
+  SmemVec s{smem + lv * padded_len<P::N>(), 1, 0};
+  auto st = op.init(plane, active ? line : 0);
   float2 v[RMAX];
+  if (active) {
 #pragma unroll
-  for (int q = 0; q < RMAX; ++q)
-    v[q] = active ? op.load(plane, line, in_elem<N, 0>(t, q)) : make_float2(0.f, 0.f);
-  if constexpr (Op::kStages >= 1) fft_run<N, Op::kInv1>(v, t, s, tw, BlockSync{});
+    for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+  } else {
+#pragma unroll
+    for (int q = 0; q < RMAX; ++q) v[q] = make_float2(0.f, 0.f);
+  }
+  if constexpr (Op::kStages >= 1) fft_run<P, Op::kInv1>(v, t, s, tw, BlockSync{});
   if constexpr (Op::kStages == 2) {
     if (active) {
 #pragma unroll
-      for (int q = 0; q < RMAX; ++q) op.mid(plane, line, out_elem<N>(t, q), v[q]);
+      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q]);
     }
-    relayout_out_to_in<N>(v, t, s, BlockSync{});
-    fft_run<N, Op::kInv2>(v, t, s, tw, BlockSync{});
+    relayout_out_to_in<P>(v, t, s, BlockSync{});
+    fft_run<P, Op::kInv2>(v, t, s, tw, BlockSync{});
   }
   typename Op::Acc acc{};
   if (active) {
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) op.store(plane, line, out_elem<N>(t, q), v[q], acc);
+    for (int q = 0; q < RMAX; ++q) op.store(st, out_elem<P>(t, q), v[q], acc);
   }
   op.finish(plane, bip, bpp, acc);
 }
 
 // Column pass. Grid: (ceil(ncols / C), nplanes); columns beyond ncols idle.
-template <int N, class Op>
-__global__ void __launch_bounds__(ColCfg<N>::THREADS) col_kernel(Op op, const float2* __restrict__ tw,
-                                                                 int ncols) {
-  constexpr int C = ColCfg<N>::C;
-  constexpr int RMAX = Plan<N>::RMAX;
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __restrict__ tw, int ncols) {
+  using P = typename S::Plan;
+  constexpr int C = S::C;
+  constexpr int RMAX = P::RMAX;
   extern __shared__ float2 smem[];
   const int c = threadIdx.x % C;
   const int t = threadIdx.x / C;
@@ -93,23 +162,28 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS) col_kernel(Op op, const fl
   const int line = blockIdx.x * C + c;
   const bool active = line < ncols;
   SmemVec s{smem, C, c};
+  auto st = op.init(plane, active ? line : 0);
   float2 v[RMAX];
+  if (active) {
 #pragma unroll
-  for (int q = 0; q < RMAX; ++q)
-    v[q] = active ? op.load(plane, line, in_elem<N, 0>(t, q)) : make_float2(0.f, 0.f);
-  if constexpr (Op::kStages >= 1) fft_run<N, Op::kInv1>(v, t, s, tw, BlockSync{});
+    for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+  } else {
+#pragma unroll
+    for (int q = 0; q < RMAX; ++q) v[q] = make_float2(0.f, 0.f);
+  }
+  if constexpr (Op::kStages >= 1) fft_run<P, Op::kInv1>(v, t, s, tw, BlockSync{});
   if constexpr (Op::kStages == 2) {
     if (active) {
 #pragma unroll
-      for (int q = 0; q < RMAX; ++q) op.mid(plane, line, out_elem<N>(t, q), v[q]);
+      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q]);
     }
-    relayout_out_to_in<N>(v, t, s, BlockSync{});
-    fft_run<N, Op::kInv2>(v, t, s, tw, BlockSync{});
+    relayout_out_to_in<P>(v, t, s, BlockSync{});
+    fft_run<P, Op::kInv2>(v, t, s, tw, BlockSync{});
   }
   typename Op::Acc acc{};
   if (active) {
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) op.store(plane, line, out_elem<N>(t, q), v[q], acc);
+    for (int q = 0; q < RMAX; ++q) op.store(st, out_elem<P>(t, q), v[q], acc);
   }
   op.finish(plane, blockIdx.x, gridDim.x, acc);
 }

@@ -1,0 +1,291 @@
+// prop_sweep.cu -- batched focus sweeps (reference: src/propagate.js:427-434)
+// and the shape autotuner.
+#include <vector>
+
+#include "ops_propagate.cuh"
+
+using namespace doe;
+
+// Pipelined focus sweep. Planes are processed in groups of G: the column pass of a
+// group (x H, inverse column FFT -> intermediate) runs on the context stream and
+// the row pass (inverse row FFT -> output) on the auxiliary stream, so the row
+// pass of group g overlaps the column pass of group g+1 and neither kernel's
+// last wave leaves SMs idle. Intermediates live in a ring of NBUF group buffers
+// sized to stay L2-resident; events order buffer reuse between the streams.
+struct SweepPipe {
+  static constexpr int NBUF = 2;
+  static constexpr int NEV = 8;  // event ring per kind (> NBUF)
+  doe_ctx* c = nullptr;
+  int nx = 0, ny = 0, G = 1;
+  long pe = 0, g = 0;  // g: groups issued so far
+  float2* wbuf = nullptr;
+
+  int init(doe_ctx* c_, int nx_, int ny_) {
+    c = c_;
+    nx = nx_;
+    ny = ny_;
+    pe = (long)nx * ny;
+    if (c->tune_sweep_group > 0) {
+      G = (int)c->tune_sweep_group;
+    } else {
+      int l2 = 0;
+      cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device);
+      const long budget = std::max<long>(l2 / 2, 1L << 20);  // NBUF buffers in half of L2
+      G = (int)std::max<long>(1, std::min<long>(kMaxGroup, budget / (NBUF * pe * (long)sizeof(float2))));
+    }
+    void* dw;
+    DOE_TRY(ensure_slot(c, kSlotW1, (size_t)NBUF * G * pe * sizeof(float2), &dw));
+    wbuf = (float2*)dw;
+    return DOE_OK;
+  }
+  cudaEvent_t ev_col(long k) { return sync_event(c, (size_t)(k % NEV)); }
+  cudaEvent_t ev_row(long k) { return sync_event(c, (size_t)(NEV + k % NEV)); }
+
+  // One field whose forward spectrum `spec` (unshifted) is resident. Planes with
+  // z == 0 are the input field itself (src/propagate.js:113), copied from the source.
+  int run_field(const float2* spec, double dx, double dy, double lambda, const double* z, int nz, int band_limit,
+                int evanescent, double soft_edge, float2* out_c64, const float2* src_c64, double* out_re,
+                double* out_im, const double* src_re, const double* src_im) {
+    for (int t0 = 0; t0 < nz; t0 += kMaxGroup) {  // one table launch per kMaxGroup distances
+      const int tn = std::min(kMaxGroup, nz - t0);
+      AsmGroupArgs a = group_args(nx, ny, dx, dy, band_limit, evanescent, soft_edge);
+      a.nplanes = tn;
+      for (int i = 0; i < tn; ++i) {
+        a.lam[i] = lambda;
+        a.z[i] = z[t0 + i];
+      }
+      AsmTables tab;
+      DOE_TRY(asm_build_tables(c, a, &tab));
+      for (int g0 = 0; g0 < tn; g0 += G, ++g) {
+        const int gn = std::min(G, tn - g0);
+        const long o0 = (long)(t0 + g0) * pe;
+        float2* w = wbuf + (g % NBUF) * (long)G * pe;
+        if (g >= NBUF) DOE_CUDA(c, cudaStreamWaitEvent(c->stream, ev_row(g - NBUF), 0));
+        DOE_TRY(with_col(c, ny, kTuneSweep, [&](auto S) {
+          return launch_col<decltype(S)>(c, ColSweep{{}, spec, w, tab, nx, ny, g0}, gn, nx);
+        }));
+        DOE_CUDA(c, cudaEventRecord(ev_col(g), c->stream));
+        DOE_CUDA(c, cudaStreamWaitEvent(c->aux, ev_col(g), 0));
+        if (out_c64) {
+          DOE_TRY(with_row(c, nx, kTuneSweep, [&](auto S) {
+            return launch_row<decltype(S)>(c, RowC64<true>{{}, w, out_c64 + o0, nx, ny, pe, pe, 1.f / (float)pe}, gn, ny,
+                                 c->aux);
+          }));
+        } else {
+          DOE_TRY(with_row(c, nx, kTuneSweep, [&](auto S) {
+            return launch_row<decltype(S)>(
+                c, RowInvToF64{{}, w, out_re + o0, out_im + o0, nx, ny, pe, 1.f / (float)pe}, gn, ny, c->aux);
+          }));
+        }
+        for (int i = 0; i < gn; ++i) {
+          if (a.z[g0 + i] != 0.0) continue;
+          const long o = o0 + (long)i * pe;
+          if (out_c64) {
+            DOE_CUDA(c, cudaMemcpyAsync(out_c64 + o, src_c64, pe * sizeof(float2), cudaMemcpyDeviceToDevice, c->aux));
+          } else {
+            DOE_CUDA(c, cudaMemcpyAsync(out_re + o, src_re, pe * sizeof(double), cudaMemcpyDeviceToDevice, c->aux));
+            DOE_CUDA(c, cudaMemcpyAsync(out_im + o, src_im, pe * sizeof(double), cudaMemcpyDeviceToDevice, c->aux));
+          }
+        }
+        DOE_CUDA(c, cudaEventRecord(ev_row(g), c->aux));
+      }
+    }
+    return DOE_OK;
+  }
+
+  // Join: the context stream waits for the last row pass.
+  int finish() {
+    if (g > 0) DOE_CUDA(c, cudaStreamWaitEvent(c->stream, ev_row(g - 1), 0));
+    return DOE_OK;
+  }
+};
+
+extern "C" int doe_asm_sweep(doe_ctx* c, const double* re, const double* im, int nx, int ny, double dx, double dy,
+                             double lambda, const double* z, int nz, int band_limit, int evanescent, double soft_edge,
+                             double* out_re, double* out_im) {
+  if (!c) return DOE_ERR_BAD_ARG;
+  DOE_TRY(check_grid(c, nx, ny, "focusSweep"));
+  if (!re || !im || !z || !out_re || !out_im || nz < 0) return set_err(c, DOE_ERR_BAD_ARG, "focusSweep: bad argument");
+  if (nz == 0) return DOE_OK;
+  const size_t n = (size_t)nx * ny;
+  void *din, *dspec, *dout;
+  DOE_TRY(ensure_slot(c, kSlotIn, 2 * n * sizeof(double), &din));
+  DOE_TRY(ensure_slot(c, kSlotW0, n * sizeof(float2), &dspec));
+  DOE_TRY(ensure_slot(c, kSlotOut, 2 * n * (size_t)nz * sizeof(double), &dout));
+  double* dre = (double*)din;
+  double* dim = dre + n;
+  float2* spec = (float2*)dspec;
+  double* ore = (double*)dout;
+  double* oim = ore + n * nz;
+  DOE_TRY(upload_f64(c, dre, re, n));
+  DOE_TRY(upload_f64(c, dim, im, n));
+  DOE_TRY(with_row0(nx, [&](auto S) {
+    return launch_row<decltype(S)>(c, RowF64In<false>{{}, dre, dim, spec, nx, ny, 0, 0}, 1, ny);
+  }));
+  DOE_TRY(with_col0(ny, [&](auto S) {
+    return launch_col<decltype(S)>(c, ColC64<false>{{}, spec, spec, nx, ny, (long)n, (long)n, 1.f}, 1, nx);
+  }));
+  SweepPipe pipe;
+  DOE_TRY(pipe.init(c, nx, ny));
+  DOE_TRY(pipe.run_field(spec, dx, dy, lambda, z, nz, band_limit, evanescent, soft_edge, nullptr, nullptr, ore, oim,
+                         dre, dim));
+  DOE_TRY(pipe.finish());
+  DOE_TRY(download_f64(c, out_re, ore, n * nz));
+  DOE_TRY(download_f64(c, out_im, oim, n * nz));
+  DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DOE_OK;
+}
+
+extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny, double dx, double dy,
+                                 const double* lambda, const double* z, int nz, int band_limit, int evanescent,
+                                 double soft_edge, void* d_out) {
+  if (!c) return DOE_ERR_BAD_ARG;
+  DOE_TRY(check_grid(c, nx, ny, "focusSweep"));
+  if (!d_fields || !lambda || !z || !d_out || nfields < 0 || nz < 0)
+    return set_err(c, DOE_ERR_BAD_ARG, "focusSweep: bad argument");
+  const long pe = (long)nx * ny;
+  void* dspec;
+  DOE_TRY(ensure_slot(c, kSlotW0, pe * sizeof(float2), &dspec));
+  float2* spec = (float2*)dspec;
+  const float2* in = (const float2*)d_fields;
+  float2* out = (float2*)d_out;
+  SweepPipe pipe;
+  DOE_TRY(pipe.init(c, nx, ny));
+  for (int f = 0; f < nfields; ++f) {
+    DOE_TRY(with_row(c, nx, kTuneFft, [&](auto S) {
+      return launch_row<decltype(S)>(c, RowC64<false>{{}, in + f * pe, spec, nx, ny, pe, pe, 1.f}, 1, ny);
+    }));
+    DOE_TRY(with_col(c, ny, kTuneFft, [&](auto S) {
+      return launch_col<decltype(S)>(c, ColC64<false>{{}, spec, spec, nx, ny, pe, pe, 1.f}, 1, nx);
+    }));
+    DOE_TRY(pipe.run_field(spec, dx, dy, lambda[f], z + (long)f * nz, nz, band_limit, evanescent, soft_edge,
+                           out + (long)f * nz * pe, in + f * pe, nullptr, nullptr, nullptr, nullptr));
+  }
+  return pipe.finish();
+}
+
+// ====================================================================== autotuner
+// Times every compiled shape variant of the plain FFT passes (kTuneFft) and of
+// the focus-sweep passes (kTuneSweep) for an nx-by-ny grid on this device and
+// keeps the fastest. Geometry (pitch, wavelength, distance) sets which
+// transfer-function path the sweep kernels take, so it is part of the input.
+// chosen[0..4] receives {fft row, fft col, sweep row, sweep col} variant indices
+// and the sweep group size.
+namespace doe {
+static int time_variant(doe_ctx* c, const std::function<int()>& launch, float* ms_out) {
+  cudaEvent_t a = prof_event(c), b = prof_event(c);  // timing-enabled events
+  struct Give {
+    doe_ctx* c;
+    cudaEvent_t a, b;
+    ~Give() {
+      c->ev_pool.push_back(a);
+      c->ev_pool.push_back(b);
+    }
+  } give{c, a, b};
+  DOE_TRY(launch());  // warm-up (also sets shared-memory attributes)
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    DOE_CUDA(c, cudaEventRecord(a, c->stream));
+    DOE_TRY(launch());
+    DOE_CUDA(c, cudaEventRecord(b, c->stream));
+    DOE_CUDA(c, cudaEventSynchronize(b));
+    float ms = 0.f;
+    DOE_CUDA(c, cudaEventElapsedTime(&ms, a, b));
+    best = std::min(best, ms);
+  }
+  *ms_out = best;
+  return DOE_OK;
+}
+}  // namespace doe
+
+extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, double lambda, double z, int* chosen) {
+  if (!c) return DOE_ERR_BAD_ARG;
+  DOE_TRY(check_grid(c, nx, ny, "autotune"));
+  const long pe = (long)nx * ny;
+  // enough planes for several waves, capped at 64 MiB per buffer
+  const int planes = (int)std::max<long>(1, std::min<long>(16, (64L << 20) / (pe * (long)sizeof(float2))));
+  void *d0, *d1;
+  DOE_TRY(ensure_slot(c, kSlotW0, pe * sizeof(float2), &d0));
+  DOE_TRY(ensure_slot(c, kSlotW1, (size_t)planes * pe * sizeof(float2), &d1));
+  float2* spec = (float2*)d0;
+  float2* w = (float2*)d1;
+  DOE_CUDA(c, cudaMemsetAsync(spec, 0, pe * sizeof(float2), c->stream));
+  DOE_CUDA(c, cudaMemsetAsync(w, 0, (size_t)planes * pe * sizeof(float2), c->stream));
+  AsmGroupArgs a = group_args(nx, ny, dx, dy, 1, 1, 0.02);
+  a.nplanes = planes;
+  for (int i = 0; i < planes; ++i) {
+    a.lam[i] = lambda;
+    a.z[i] = z * (1.0 + 0.01 * i);
+  }
+  AsmTables tab;
+  DOE_TRY(asm_build_tables(c, a, &tab));
+  const int lx = ilog2i(nx), ly = ilog2i(ny);
+  int pick[4] = {0, 0, 0, 0};
+  const int nrow = row_variant_count(nx), ncol = col_variant_count(ny);
+  for (int kind : {(int)kTuneFft, (int)kTuneSweep}) {
+    float best = 1e30f;
+    for (int v = 0; v < nrow; ++v) {
+      c->tune_row[kind][lx] = (unsigned char)v;
+      float ms;
+      DOE_TRY(time_variant(c, [&]() {
+        return with_row(c, nx, kind, [&](auto S) {
+          return launch_row<decltype(S)>(c, RowC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, ny);
+        });
+      }, &ms));
+      if (ms < best) {
+        best = ms;
+        pick[kind == kTuneFft ? 0 : 2] = v;
+      }
+    }
+    c->tune_row[kind][lx] = (unsigned char)pick[kind == kTuneFft ? 0 : 2];
+    best = 1e30f;
+    for (int v = 0; v < ncol; ++v) {
+      c->tune_col[kind][ly] = (unsigned char)v;
+      float ms;
+      DOE_TRY(time_variant(c, [&]() {
+        return with_col(c, ny, kind, [&](auto S) {
+          if (kind == kTuneSweep) return launch_col<decltype(S)>(c, ColSweep{{}, spec, w, tab, nx, ny, 0}, planes, nx);
+          return launch_col<decltype(S)>(c, ColC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, nx);
+        });
+      }, &ms));
+      if (ms < best) {
+        best = ms;
+        pick[kind == kTuneFft ? 1 : 3] = v;
+      }
+    }
+    c->tune_col[kind][ly] = (unsigned char)pick[kind == kTuneFft ? 1 : 3];
+  }
+  // planes per launch pair of the pipelined sweep: time one 64-distance field
+  {
+    const int nz = 64;
+    std::vector<double> zs(nz);
+    for (int i = 0; i < nz; ++i) zs[i] = z * (1.0 + 0.01 * i);
+    void* dout;
+    DOE_TRY(ensure_slot(c, kSlotOut, (size_t)nz * pe * sizeof(float2), &dout));
+    float best = 1e30f;
+    long bestG = 0;
+    const long saved = c->tune_sweep_group;
+    for (long G : {4L, 8L, 16L, 32L, 64L}) {
+      if ((size_t)G * pe * sizeof(float2) * SweepPipe::NBUF > ((size_t)1 << 31)) break;
+      c->tune_sweep_group = G;
+      float ms;
+      DOE_TRY(time_variant(c, [&]() {
+        SweepPipe pipe;
+        DOE_TRY(pipe.init(c, nx, ny));
+        DOE_TRY(pipe.run_field(spec, dx, dy, lambda, zs.data(), nz, 1, 1, 0.02, (float2*)dout, spec, nullptr,
+                               nullptr, nullptr, nullptr));
+        return pipe.finish();
+      }, &ms));
+      if (ms < best) {
+        best = ms;
+        bestG = G;
+      }
+    }
+    c->tune_sweep_group = saved > 0 ? saved : bestG;
+  }
+  if (chosen) {
+    for (int k = 0; k < 4; ++k) chosen[k] = pick[k];
+    chosen[4] = (int)c->tune_sweep_group;
+  }
+  return DOE_OK;
+}

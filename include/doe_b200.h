@@ -62,6 +62,26 @@ int doe_ctx_synchronize(doe_ctx* ctx);
 int doe_host_alloc(doe_ctx* ctx, void** ptr, unsigned long long bytes);
 int doe_host_free(doe_ctx* ctx, void* ptr);
 
+/* Instrumentation (engine-only; no reference counterpart). */
+unsigned long long doe_ctx_launch_count(doe_ctx* ctx); /* kernels launched so far */
+int doe_ctx_set_profiling(doe_ctx* ctx, int on); /* bracket each launch with events */
+/* Per-kernel totals since the last read: returns the number of labels written
+ * (names: max_entries rows of name_len chars). Synchronises the stream. */
+int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_len,
+                         double* total_ms, unsigned long long* count);
+
+/* Tuning knobs (engine-only): "sweep_group" = planes per focus-sweep launch pair
+ * (0 = sized from the L2 cache); "fft_row", "fft_col", "sweep_row", "sweep_col",
+ * "design_row", "design_col" = (log2(n) << 8) | shape variant for that pass. */
+int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
+/* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
+ * nx-by-ny grid at the given geometry on this device and keeps the fastest for
+ * the plain FFT and focus-sweep passes, then times the pipelined sweep for
+ * several group sizes ("sweep_group"). chosen (5 ints, may be NULL) receives the
+ * picked {fft row, fft column, sweep row, sweep column} variants and group size. */
+int doe_autotune(doe_ctx* ctx, int nx, int ny, double dx, double dy, double lambda, double z,
+                 int* chosen);
+
 /* ------------------------------------------------------------ transforms */
 /* fft2d(re, im, nx, ny, inverse) -- src/fft.js:148-154. In place; forward
  * unscaled, inverse scaled by 1/(nx*ny). */
