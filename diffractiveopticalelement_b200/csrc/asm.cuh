@@ -214,18 +214,21 @@ inline int asm_tables_bytes(int nplanes, int nx, int ny, size_t* bytes) {
   return 0;
 }
 
+// Layout from a 256-byte-aligned base: plane scalars (rounded to 256 B), then the
+// 16-byte AxisBin arrays, then the FP64 arrays, so every array keeps its natural
+// alignment whatever nx and ny are (including axes of length 1).
 inline AsmTables asm_tables_carve(void* base, int nplanes, int nx, int ny) {
   char* p = (char*)base;
   AsmTables t;
   t.pl = (AsmPlane*)p;
   p += ((sizeof(AsmPlane) * nplanes + 255) / 256) * 256;
-  t.xf2 = (double*)p;
-  p += sizeof(double) * nx;
-  t.yf2 = (double*)p;
-  p += sizeof(double) * ny;
   t.xt = (AxisBin*)p;
   p += sizeof(AxisBin) * (size_t)nplanes * nx;
   t.yt = (AxisBin*)p;
+  p += sizeof(AxisBin) * (size_t)nplanes * ny;
+  t.xf2 = (double*)p;
+  p += sizeof(double) * nx;
+  t.yf2 = (double*)p;
   return t;
 }
 

@@ -71,7 +71,8 @@ def test_asm_matches_oracle(engine, oracle, n, dx, z, bl, ev, se):
     assert np.array_equal(f.re, re) and np.array_equal(f.im, im)  # clone semantics
 
 
-@pytest.mark.parametrize("nx,ny,dx,dy", [(256, 64, 8e-6, 6e-6), (16, 1024, 4e-6, 4e-6)])
+@pytest.mark.parametrize("nx,ny,dx,dy", [(256, 64, 8e-6, 6e-6), (16, 1024, 4e-6, 4e-6), (1, 64, 8e-6, 8e-6),
+                                         (128, 1, 8e-6, 8e-6), (1, 1, 8e-6, 8e-6)])
 def test_asm_rectangular_grid(engine, oracle, nx, ny, dx, dy):
     re, im = rand_planes(nx * ny, 7)
     f = engine.ComplexField(nx, ny, dx, dy)
