@@ -64,6 +64,7 @@ def _declare(L):
         "doe_focal_plane": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, _dp, _dp, _dp]),
         "doe_fft2d_dev": (i, [ctxp, _vp, i, i, i, i]),
         "doe_asm_sweep_dev": (i, [ctxp, _vp, i, i, i, d, d, _dp, _dp, i, i, i, d, _vp]),
+        "doe_asm_c64_noalloc": (i, [_vp, _vp, i, i, d, d, d, d, i, i, d, _vp, C.c_char_p, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)

@@ -122,6 +122,23 @@ int doe_asm_sweep_dev(doe_ctx* ctx, const void* d_fields, int nfields, int nx, i
                       double dx, double dy, const double* lambda, const double* z, int nz,
                       int band_limit, int evanescent, double soft_edge, void* d_out);
 
+/* ------------------------------------------------------------ allocation-free */
+/* No counterpart in the reference. Angular-spectrum propagation of one complex64
+ * plane for callers that must not allocate device memory (a host runtime that owns
+ * every device allocation, or a latency-critical loop that cannot afford the
+ * allocator's implicit synchronisation). The caller passes device input and
+ * output planes (they may alias) and a CUDA stream (NULL = default stream); the
+ * routine needs no context and allocates nothing: its scratch is a fixed
+ * 2.6 MiB array that every GPU loading this library holds until exit. Limit:
+ * nx*ny <= 262144 samples (e.g. 512x512), each axis <= 8192; larger grids return
+ * DOE_ERR_UNSUPPORTED. The first call on a device sets the scratch up and
+ * synchronises the stream once; make it before any stream capture. Calls whose
+ * work overlaps on the GPU share the scratch and race: serialise them. The error
+ * message, if any, is written to err (err_len bytes, may be NULL). */
+int doe_asm_c64_noalloc(const void* d_in, void* d_out, int nx, int ny, double dx, double dy,
+                        double lambda, double z, int band_limit, int evanescent,
+                        double soft_edge, void* stream, char* err, int err_len);
+
 #ifdef __cplusplus
 }
 #endif
