@@ -7,7 +7,10 @@ sm_100a CUDA kernels behind the C ABI in include/doe_b200.h
 """
 from ._lib import DOEError, EngineUnavailable, Context, context, load_library
 from .fft import fft2d, fft2dOut, isPow2, nextPow2
-from .field import ComplexField
+from .field import ComplexField, discMask, rectMask, ringMask
+from .doe import (DEFAULT_DESIGN, blurRaster, designDOE, flatPhase, fourierCgh, gerchbergSaxton,
+                  gerchbergSaxtonMultiPlane, illuminationProfile, kinoformLens, makeRng, prepareTargetAmp,
+                  randomPhase, weightedGerchbergSaxton, wrapPhase)
 from .propagate import (
     DEFAULT_WAVELENGTH,
     angularSpectrumTransferFunction,
@@ -25,5 +28,7 @@ __all__ = [
     "fft2d", "fft2dOut", "isPow2", "nextPow2", "ComplexField",
     "DEFAULT_WAVELENGTH", "angularSpectrumTransferFunction", "focalPlaneSpectrum", "focusSweep",
     "fresnelMinDistance", "localFrequencyLimit", "propagate", "propagateAngularSpectrum",
-    "propagateAngularSpectrumInPlace",
+    "propagateAngularSpectrumInPlace", "discMask", "rectMask", "ringMask", "DEFAULT_DESIGN", "blurRaster",
+    "designDOE", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
+    "kinoformLens", "makeRng", "prepareTargetAmp", "randomPhase", "weightedGerchbergSaxton", "wrapPhase",
 ]

@@ -41,6 +41,31 @@ class EngineUnavailable(RuntimeError):
 
 _dp = C.POINTER(C.c_double)
 _vp = C.c_void_p
+
+DOE_ALG_GS, DOE_ALG_WGS, DOE_ALG_FOURIER, DOE_ALG_WGS_FOURIER = 0, 1, 2, 3
+
+
+class DesignDesc(C.Structure):
+    """doe_design_desc (include/doe_b200.h)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("lambda_", C.c_double), ("z", C.c_double), ("algorithm", C.c_int), ("iterations", C.c_int),
+                ("feedback", C.c_double), ("escape", C.c_int), ("beta", C.c_double), ("seed", C.c_double),
+                ("illumination", _dp), ("target_amp", _dp), ("roi", _dp), ("init_phase", _dp)]
+
+
+class DesignResult(C.Structure):
+    """doe_design_result."""
+    _fields_ = [("phase", _dp), ("amplitude", _dp), ("intensity", _dp), ("error", _dp),
+                ("efficiency", _dp), ("weights", _dp), ("rmse", C.c_double)]
+
+
+class DesignDevDesc(C.Structure):
+    """doe_design_dev_desc (device-resident FP32 planes)."""
+    _fields_ = [("batch", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("lambda_", C.c_double), ("z", C.c_double), ("lambdas", _dp), ("zs", _dp),
+                ("algorithm", C.c_int), ("iterations", C.c_int), ("feedback", C.c_double), ("escape", C.c_int),
+                ("beta", C.c_double), ("illumination", _vp), ("target_amp", _vp), ("roi", _vp), ("phase", _vp),
+                ("amplitude", _vp), ("weights", _vp), ("error", _vp), ("efficiency", _vp), ("rmse", _vp)]
 _lib = None
 _lock = threading.Lock()
 
@@ -65,6 +90,15 @@ def _declare(L):
         "doe_fft2d_dev": (i, [ctxp, _vp, i, i, i, i]),
         "doe_asm_sweep_dev": (i, [ctxp, _vp, i, i, i, d, d, _dp, _dp, i, i, i, d, _vp]),
         "doe_asm_c64_noalloc": (i, [_vp, _vp, i, i, d, d, d, d, i, i, d, _vp, C.c_char_p, i]),
+        "doe_design": (i, [ctxp, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
+        "doe_random_phase": (i, [i, i, d, _dp]),
+        "doe_design_batch": (i, [ctxp, i, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
+        "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
+        "doe_multiplane": (i, [ctxp, i, i, d, d, d, _dp, i, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]),
+        "doe_autotune": (i, [ctxp, i, i, d, d, d, d, C.POINTER(C.c_int)]),
+        "doe_ctx_set_tuning": (i, [ctxp, C.c_char_p, C.c_longlong]),
+        "doe_ctx_launch_count": (C.c_ulonglong, [ctxp]),
+        "doe_ctx_set_profiling": (i, [ctxp, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)

@@ -1,0 +1,536 @@
+// design_ops.cuh -- fused operators of the Gerchberg-Saxton family
+// (reference: src/doe.js:327-437 gerchbergSaxton, :455-546 weightedGerchbergSaxton,
+// :557-626 gerchbergSaxtonMultiPlane, :639-730 fourierCgh).
+//
+// A batch of B designs of one grid size runs as one launch per pass: the plane
+// index of the row/column kernels is the design index. Per-pixel arrays are FP32
+// ([B][nx*ny], centred layout idx = x + y*nx exactly as the reference's planes);
+// every reduction (error, efficiency, power, RMSE, weight normalisation)
+// accumulates in FP64 and is folded per design by the last CTA of that design
+// (fixed order, deterministic), which also updates the design's scalar state.
+#pragma once
+#include "ops_propagate.cuh"
+
+namespace doe {
+
+// Per-design scalars carried across passes (device memory).
+struct DesignState {
+  double norm;      // WGS: weights = w_raw * norm
+  double best;      // WGS: best unweighted ROI RMSE so far
+  double eff_cur;   // image-plane WGS: efficiency of the current forward field
+  double pad;
+};
+
+enum RedSlot { kErrNum = 0, kErrDen, kInRoi, kTotal, kRmseNum, kRmseDen, kWsum, kTsum, kRedK };
+using DesignAcc = DAcc<kRedK>;
+
+struct DesignBufs {
+  int nx, ny, iters;
+  double dx, dy;
+  float feedback;   // HIO feedback (0 = plain GS)
+  int escape;       // iterations before the feedback applies
+  float beta;       // WGS exponent
+  const float* illum;   // [B][n] amplitude A
+  const float* tgt;     // [B][n] target amplitude t (plane 0 of a multi-plane set)
+  const float* roi;     // [B][n] soft ROI m, or null (1 everywhere)
+  long tgt_stride;      // elements between designs in tgt / roi
+  float* wraw;          // [B][n] WGS weights before normalisation, or null
+  float* phase;         // [B][n] DOE phase
+  float* best_phase;    // [B][n] WGS best iterate
+  float* amp;           // [B][n] amplitude of the current forward field
+  float* best_amp;      // [B][n]
+  float2* U;            // [B][n] target-plane field (image-plane WGS)
+  float2* W;            // [B][n] work
+  const float2* htab;   // transfer function in FFT bin order
+  long htab_stride;     // elements between designs (0: shared geometry)
+  DesignState* st;      // [B]
+  double* err_hist;     // [B][iters]
+  double* eff_hist;     // [B][iters]
+  double* pp_err;       // multi-plane: [B][nplanes][iters]
+  int mp_plane, mp_nplanes;
+  unsigned char* improved;  // [B][iters]
+  double* partials;     // [B][max blocks][kRedK]
+  unsigned* counters;   // [B]
+  double* totals;       // [B][kRedK]
+  __device__ __forceinline__ long pe() const { return (long)nx * ny; }
+};
+
+__device__ __forceinline__ int rotn(int i, int n) { return (i + (n >> 1)) & (n - 1); }
+
+__device__ __forceinline__ float2 unit_phasor(float2 v) {
+  const float r2 = v.x * v.x + v.y * v.y;
+  if (r2 > 0.f) {
+    const float inv = rsqrtf(r2);
+    return make_float2(v.x * inv, v.y * inv);
+  }
+  return make_float2(1.f, 0.f);  // atan2(0, 0) = 0
+}
+
+// Fold one design's block sums; returns true in the last block (totals valid).
+__device__ __forceinline__ bool design_reduce(const DesignBufs& b, int p, int bip, int bpp, DesignAcc& acc) {
+  return group_reduce<kRedK>(acc, p, bip, bpp, b.partials, b.counters, b.totals);
+}
+
+// ------------------------------------------------------------------ column passes
+// Image-plane propagation column pass with a tabulated transfer function:
+// forward column FFT, x H (+z) or conj(H) (-z), inverse column FFT, in place.
+template <bool CONJ>
+struct ColAsmTab : NoReduce {
+  static constexpr const char* kName = CONJ ? "design_col_back" : "design_col_fwd";
+  static constexpr int kStages = 2;
+  static constexpr bool kInv1 = false, kInv2 = true;
+  float2* w;
+  const float2* htab;
+  long htab_stride;
+  int nx, ny;
+  struct State {
+    float2* w;
+    const float2* h;
+  };
+  __device__ __forceinline__ State init(int p, int x) const {
+    return {w + p * (long)nx * ny + x, htab + p * htab_stride + x};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int y) const { return s.w[(long)y * nx]; }
+  __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc&) const {
+    const float2 h = __ldg(&s.h[(long)y * nx]);
+    v = CONJ ? cmulc(v, h) : cmul(v, h);
+  }
+  __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const { s.w[(long)y * nx] = v; }
+};
+
+// Fourier-domain column pass (src/doe.js:666-717): forward column FFT, unitary
+// scale, measurement, WGS weight update, amplitude constraint, inverse column
+// FFT. Bin (kx, ky) holds the centred sample (rot(kx), rot(ky)).
+template <bool WGS>
+struct ColFourier {
+  static constexpr const char* kName = WGS ? "design_col_fourier_wgs" : "design_col_fourier";
+  static constexpr int kStages = 2;
+  static constexpr bool kInv1 = false, kInv2 = true;
+  using Acc = DesignAcc;
+  DesignBufs b;
+  int it;
+  float norm;  // 1/sqrt(nx ny)
+  struct State {
+    const float* t;
+    const float* m;
+    float* w;
+    float* amp;
+    float2* W;
+    float wn;   // weight normalisation of this pass
+  };
+  __device__ __forceinline__ State init(int p, int x) const {
+    const long o = p * b.pe() + rotn(x, b.nx);
+    const long ot = p * b.tgt_stride + rotn(x, b.nx);
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, WGS ? b.wraw + o : nullptr, b.amp + o,
+            b.W + p * b.pe() + x, WGS ? (float)b.st[p].norm : 1.f};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int y) const { return s.W[(long)y * b.nx]; }
+  __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc& acc) const {
+    const long j = (long)rotn(y, b.ny) * b.nx;
+    v = cscale(v, norm);
+    const float a = sqrtf(v.x * v.x + v.y * v.y);
+    const double ad = a;
+    s.amp[j] = a;
+    const float m = s.m ? s.m[j] : 1.f;
+    const float t0 = s.t[j];
+    float w = 1.f;
+    if constexpr (WGS) w = s.w[j] * s.wn;
+    const float tw = t0 * w;
+    acc.v[kTotal] += ad * ad;
+    if (m > 0.f) {
+      acc.v[kInRoi] += ad * ad * m;
+      const double d = (ad - (double)tw) * m;
+      acc.v[kErrNum] += d * d;
+      acc.v[kErrDen] += (double)tw * tw;
+    }
+    if constexpr (WGS) {
+      if (m > 0.f) {  // src/doe.js:489-524 on the amplitude of this forward pass
+        const double d = ad - (double)t0;
+        acc.v[kRmseNum] += d * d;
+        acc.v[kRmseDen] += (double)t0 * t0;
+        const float ratio = a > 1e-30f ? t0 / a : 2.f;
+        float wn = w * powf(fminf(fmaxf(ratio, 0.25f), 4.f), b.beta);
+        wn = fminf(fmaxf(wn, 1e-4f), 1e4f);
+        s.w[j] = wn;  // stored before normalisation
+        acc.v[kWsum] += (double)wn * wn * t0 * t0;
+        acc.v[kTsum] += (double)t0 * t0;
+      }
+    }
+    // constraint: target inside the ROI, measured modulus outside
+    const float tc = m > 0.f ? tw : a;
+    if (a > 0.f) {
+      v = cscale(v, tc / a);
+    } else {
+      v = make_float2(tc, 0.f);
+    }
+  }
+  __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const { s.W[(long)y * b.nx] = v; }
+  __device__ __forceinline__ void finish(int p, int bip, int bpp, Acc& acc) const {
+    if (!design_reduce(b, p, bip, bpp, acc) || threadIdx.x != 0) return;
+    const double* T = b.totals + (long)p * kRedK;
+    const double err = T[kErrDen] > 0 ? sqrt(T[kErrNum] / T[kErrDen]) : 0.0;
+    const double eff = T[kTotal] > 0 ? T[kInRoi] / T[kTotal] : 0.0;
+    const long h = (long)p * b.iters + it;
+    b.eff_hist[h] = eff;
+    if constexpr (WGS) {
+      DesignState& S = b.st[p];
+      const double rmse = T[kRmseDen] > 0 ? sqrt(T[kRmseNum] / T[kRmseDen]) : 0.0;
+      const bool imp = rmse < S.best;
+      if (imp) S.best = rmse;
+      b.improved[h] = imp ? 1 : 0;
+      b.err_hist[h] = S.best;
+      S.norm = T[kWsum] > 0 ? sqrt(T[kTsum] / T[kWsum]) : 1.0;
+    } else {
+      b.err_hist[h] = err;
+    }
+  }
+};
+
+// ------------------------------------------------------------------ row passes
+// Forward row pass from the DOE phase: A exp(i phi) -> forward row FFT -> W.
+// ROT reads the centred phase at the rotated index (ifftshift of the Fourier loop).
+template <bool ROT>
+struct RowDoeFwd : NoReduce {
+  static constexpr const char* kName = "design_row_doe_fwd";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = false, kInv2 = false;
+  DesignBufs b;
+  struct State {
+    const float* A;
+    const float* ph;
+    float2* w;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long pe = b.pe();
+    const int ys = ROT ? rotn(y, b.ny) : y;
+    return {b.illum + p * pe + (long)ys * b.nx, b.phase + p * pe + (long)ys * b.nx, b.W + p * pe + (long)y * b.nx};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const {
+    const int xs = ROT ? rotn(x, b.nx) : x;
+    float sn, cs;
+    sincosf(s.ph[xs], &sn, &cs);
+    const float a = s.A[xs];
+    return make_float2(a * cs, a * sn);
+  }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.w[x] = v; }
+};
+
+// End of a back-propagation (or inverse Fourier transform) and start of the next
+// forward one: inverse row FFT of W gives the DOE-plane field, its argument
+// becomes the new DOE phase (src/doe.js:401-410, :718-722), the illumination
+// amplitude is re-imposed (A v/|v| = A exp(i atan2(v))) and, when FWD, the
+// forward row FFT of the next propagation is taken. ROT stores at the rotated
+// (fftshift) index. SNAP copies the phase and the forward amplitude into the
+// best-iterate buffers when the last reduction flagged an improvement.
+template <bool FWD, bool ROT, bool SNAP>
+struct RowDoeUpdate : NoReduce {
+  static constexpr const char* kName = FWD ? "design_row_doe_update" : "design_row_doe_last";
+  static constexpr int kStages = FWD ? 2 : 1;
+  static constexpr bool kInv1 = true, kInv2 = false;
+  DesignBufs b;
+  int snap_it;  // iteration whose improvement flag is consulted (SNAP)
+  struct State {
+    const float* A;
+    float* ph;
+    float* bph;
+    const float* amp;
+    float* bamp;
+    float2* w;
+    bool snap;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long pe = b.pe();
+    const long o = p * pe + (long)(ROT ? rotn(y, b.ny) : y) * b.nx;
+    bool snap = false;
+    if constexpr (SNAP) snap = b.improved[(long)p * b.iters + snap_it] != 0;
+    return {b.illum + o, b.phase + o, SNAP ? b.best_phase + o : nullptr, SNAP ? b.amp + o : nullptr,
+            SNAP ? b.best_amp + o : nullptr, b.W + p * pe + (long)y * b.nx, snap};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
+  __device__ __forceinline__ float2 doe(const State& s, int x, float2 v) const {
+    const int xi = ROT ? rotn(x, b.nx) : x;
+    const float ph = atan2f(v.y, v.x);
+    s.ph[xi] = ph;
+    if constexpr (SNAP) {
+      if (s.snap) {
+        s.bph[xi] = ph;
+        s.bamp[xi] = s.amp[xi];
+      }
+    }
+    const float2 u = unit_phasor(v);
+    const float a = s.A[xi];
+    return make_float2(a * u.x, a * u.y);
+  }
+  __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc&) const { v = doe(s, x, v); }
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const {
+    if constexpr (FWD) {
+      s.w[x] = v;
+    } else {
+      (void)doe(s, x, v);
+    }
+  }
+};
+
+// Target plane of plain GS / HIO and of one multi-plane step (src/doe.js:355-397,
+// :579-611): the inverse row FFT gives the forward field U of the current phase;
+// its error and efficiency are measured (FP64), the amplitude constraint is applied
+// and the forward row FFT of the back-propagation is taken. FINAL only measures the
+// field and stores its amplitude (the reference's final forward pass, :418-426).
+// MP selects the multi-plane error definition and per-plane history.
+template <bool FINAL, bool MP>
+struct RowGsTarget {
+  static constexpr const char* kName = FINAL ? "design_row_gs_final" : "design_row_gs_target";
+  static constexpr int kStages = FINAL ? 1 : 2;
+  static constexpr bool kInv1 = true, kInv2 = false;
+  using Acc = DesignAcc;
+  DesignBufs b;
+  int it;
+  float scale;  // 1/(nx ny)
+  struct State {
+    const float* t;
+    const float* m;
+    float* amp;
+    float2* w;
+    float fb;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * b.pe() + (long)y * b.nx;
+    const long ot = p * b.tgt_stride + (long)y * b.nx;
+    const float fb = (!MP && it >= b.escape) ? b.feedback : 0.f;
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.amp + o, b.W + o, fb};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
+  __device__ __forceinline__ float measure(const State& s, int x, float2 u, Acc& acc) const {
+    const float a = sqrtf(u.x * u.x + u.y * u.y);
+    const double ad = a, i2 = ad * ad;
+    const float m = s.m ? s.m[x] : 1.f;
+    const double t = s.t[x];
+    acc.v[kTotal] += i2;
+    if (m > 0.f) {
+      acc.v[kInRoi] += i2 * m;
+      if constexpr (MP) {
+        const double d = (ad - t) * m;
+        acc.v[kErrNum] += d * d;
+        acc.v[kErrDen] += t * t;
+      } else if (t > 0.0 || i2 > 0.0) {
+        const double d = ad * m - t * m;
+        acc.v[kErrNum] += d * d;
+        acc.v[kErrDen] += t * t;
+      }
+    }
+    return a;
+  }
+  __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc& acc) const {
+    const float2 u = cscale(v, scale);
+    const float a = measure(s, x, u, acc);
+    const float m = s.m ? s.m[x] : 1.f;
+    const float t = s.t[x];
+    float na;
+    if (m > 0.f) {
+      na = t;
+      if (s.fb > 0.f && a > 0.f) na = t + s.fb * (a - t);
+    } else {
+      na = a * (1.f - s.fb) + s.fb * a;
+    }
+    v = a > 0.f ? cscale(u, na / a) : u;
+  }
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc& acc) const {
+    if constexpr (FINAL) {
+      const float2 u = cscale(v, scale);
+      s.amp[x] = measure(s, x, u, acc);
+    } else {
+      s.w[x] = v;
+    }
+  }
+  __device__ __forceinline__ void finish(int p, int bip, int bpp, Acc& acc) const {
+    if constexpr (FINAL) return;  // the final pass only delivers the amplitude
+    if (!design_reduce(b, p, bip, bpp, acc) || threadIdx.x != 0) return;
+    const double* T = b.totals + (long)p * kRedK;
+    const double err = T[kErrDen] > 0 ? sqrt(T[kErrNum] / T[kErrDen]) : 0.0;
+    if constexpr (MP) {
+      b.pp_err[((long)p * b.mp_nplanes + b.mp_plane) * b.iters + it] = err;
+    } else {
+      const long h = (long)p * b.iters + it;
+      b.err_hist[h] = err;
+      b.eff_hist[h] = T[kTotal] > 0 ? (T[kInRoi] * b.dx * b.dy) / (T[kTotal] * b.dx * b.dy) : 0.0;
+    }
+  }
+};
+
+// Image-plane WGS, end of an iteration (src/doe.js:417-426 then :489-529): the
+// inverse row FFT gives the forward field U of the new phase, stored for the next
+// constraint; FP64 sums of the unweighted ROI RMSE, of the efficiency of U and of
+// the weight update (w <- clamp(w clamp(t/a, 1/4, 4)^beta, 1e-4, 1e4), stored
+// before normalisation). The last CTA of a design records the histories, the best
+// RMSE and the new normalisation sqrt(sum t^2 / sum w^2 t^2). INITIAL only
+// measures the efficiency of the first forward field.
+template <bool INITIAL>
+struct RowWgsTarget {
+  static constexpr const char* kName = INITIAL ? "design_row_wgs_first" : "design_row_wgs_target";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = true, kInv2 = false;
+  using Acc = DesignAcc;
+  DesignBufs b;
+  int it;
+  float scale;
+  struct State {
+    const float* t;
+    const float* m;
+    float* w;
+    float2* U;
+    const float2* W;
+    float wn;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * b.pe() + (long)y * b.nx;
+    const long ot = p * b.tgt_stride + (long)y * b.nx;
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, (float)b.st[p].norm};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const { return s.W[x]; }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc& acc) const {
+    const float2 u = cscale(v, scale);
+    s.U[x] = u;
+    const float a = sqrtf(u.x * u.x + u.y * u.y);
+    const double ad = a, i2 = ad * ad;
+    const float m = s.m ? s.m[x] : 1.f;
+    acc.v[kTotal] += i2;
+    if (m > 0.f) acc.v[kInRoi] += i2 * m;
+    if constexpr (!INITIAL) {
+      if (m > 0.f) {
+        const float t = s.t[x];
+        const double d = ad - (double)t;
+        acc.v[kRmseNum] += d * d;
+        acc.v[kRmseDen] += (double)t * t;
+        const float ratio = a > 1e-30f ? t / a : 2.f;
+        float w = s.w[x] * s.wn * powf(fminf(fmaxf(ratio, 0.25f), 4.f), b.beta);
+        w = fminf(fmaxf(w, 1e-4f), 1e4f);
+        s.w[x] = w;
+        acc.v[kWsum] += (double)w * w * t * t;
+        acc.v[kTsum] += (double)t * t;
+      }
+    }
+  }
+  __device__ __forceinline__ void finish(int p, int bip, int bpp, Acc& acc) const {
+    if (!design_reduce(b, p, bip, bpp, acc) || threadIdx.x != 0) return;
+    const double* T = b.totals + (long)p * kRedK;
+    DesignState& S = b.st[p];
+    const double eff = T[kTotal] > 0 ? (T[kInRoi] * b.dx * b.dy) / (T[kTotal] * b.dx * b.dy) : 0.0;
+    if constexpr (INITIAL) {
+      S.eff_cur = eff;
+    } else {
+      const long h = (long)p * b.iters + it;
+      const double rmse = T[kRmseDen] > 0 ? sqrt(T[kRmseNum] / T[kRmseDen]) : 0.0;
+      const bool imp = rmse < S.best;
+      if (imp) S.best = rmse;
+      b.improved[h] = imp ? 1 : 0;
+      b.err_hist[h] = S.best;
+      b.eff_hist[h] = S.eff_cur;
+      S.eff_cur = eff;
+      S.norm = T[kWsum] > 0 ? sqrt(T[kTsum] / T[kWsum]) : 1.0;
+    }
+  }
+};
+
+// Image-plane WGS, start of an iteration (src/doe.js:380-397 with weights): load
+// the stored forward field U, apply the constraint with t * w_raw * norm inside the
+// ROI (outside: unchanged), forward row FFT of the back-propagation. When the
+// previous iteration improved the best RMSE, its phase and amplitude are copied
+// into the best-iterate buffers on the way.
+struct RowWgsConstrain : NoReduce {
+  static constexpr const char* kName = "design_row_wgs_constrain";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = false, kInv2 = false;
+  DesignBufs b;
+  int snap_it;  // -1: no snapshot check
+  struct State {
+    const float* t;
+    const float* m;
+    const float* w;
+    const float2* U;
+    float2* W;
+    const float* ph;
+    float* bph;
+    float* bamp;
+    float wn;
+    bool snap;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * b.pe() + (long)y * b.nx;
+    const long ot = p * b.tgt_stride + (long)y * b.nx;
+    const bool snap = snap_it >= 0 && b.improved[(long)p * b.iters + snap_it] != 0;
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, b.phase + o,
+            b.best_phase + o, b.best_amp + o, (float)b.st[p].norm, snap};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const {
+    const float2 u = s.U[x];
+    const float a = sqrtf(u.x * u.x + u.y * u.y);
+    if (s.snap) {
+      s.bph[x] = s.ph[x];
+      s.bamp[x] = a;
+    }
+    const float m = s.m ? s.m[x] : 1.f;
+    if (m > 0.f && a > 0.f) return cscale(u, (s.t[x] * (s.w[x] * s.wn)) / a);
+    return u;
+  }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.W[x] = v; }
+};
+
+// Design loops are compiled for power-of-two axes 32..4096 with the default CTA
+// shapes (each operator is instantiated once per size).
+constexpr int kDesignMinN = 32, kDesignMaxN = 4096;
+
+template <class F>
+inline int with_design_n(int n, F&& f) {
+  switch (n) {
+    case 32: return f(std::integral_constant<int, 32>{});
+    case 64: return f(std::integral_constant<int, 64>{});
+    case 128: return f(std::integral_constant<int, 128>{});
+    case 256: return f(std::integral_constant<int, 256>{});
+    case 512: return f(std::integral_constant<int, 512>{});
+    case 1024: return f(std::integral_constant<int, 1024>{});
+    case 2048: return f(std::integral_constant<int, 2048>{});
+    case 4096: return f(std::integral_constant<int, 4096>{});
+    default: return DOE_ERR_UNSUPPORTED;
+  }
+}
+template <class Op>
+inline int design_row(doe_ctx* c, const Op& op, int B, int nx, int ny) {
+  return with_design_n(nx, [&](auto NC) {
+    return launch_row<typename DefRow<decltype(NC)::value>::type>(c, op, B, ny);
+  });
+}
+template <class Op>
+inline int design_col(doe_ctx* c, const Op& op, int B, int nx, int ny) {
+  return with_design_n(ny, [&](auto NC) {
+    return launch_col<typename DefCol<decltype(NC)::value>::type>(c, op, B, nx);
+  });
+}
+inline int design_bpp(int nx, int ny) {
+  int bpp = 1;
+  with_design_n(nx, [&](auto NC) {
+    using S = typename DefRow<decltype(NC)::value>::type;
+    bpp = std::max(bpp, (ny + S::V - 1) / S::V);
+    return 0;
+  });
+  with_design_n(ny, [&](auto NC) {
+    using S = typename DefCol<decltype(NC)::value>::type;
+    bpp = std::max(bpp, (nx + S::C - 1) / S::C);
+    return 0;
+  });
+  return bpp;
+}
+
+// Pass sequences, one translation unit each (design_gs.cu, design_wgs.cu,
+// design_fourier.cu); the state in `b` is initialised by the caller.
+int design_run_gs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
+int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
+int design_run_fourier(doe_ctx* c, const DesignBufs& b, int B, int iterations, bool wgs);
+// Multi-plane (one design): plane p uses transfer table htab + p*n and target /
+// ROI planes tgt0 + p*n, roi0 + p*n (roi0 may be null).
+int design_run_multiplane(doe_ctx* c, DesignBufs b, int iterations, int nplanes, const float2* htab,
+                          const float* tgt0, const float* roi0);
+
+}  // namespace doe

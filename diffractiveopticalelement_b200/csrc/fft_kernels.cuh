@@ -8,7 +8,7 @@
 //   kInv1, kInv2       direction of each transform
 //   State init(plane, line)                         per-thread invariants of a line
 //   load(State&, e)                 -> float2        input element e of the line
-//   mid(State&, e, float2&)                          pointwise op between stages
+//   mid(State&, e, float2&, Acc&)                    pointwise op between stages
 //   store(State&, e, float2, Acc&)                   consume output element e
 //   finish(plane, block_in_plane, blocks_per_plane, Acc&)   block epilogue
 // `line` is the row index y for the row kernel and the column index x for the
@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __
   const bool active = line < nlines;
   SmemVec s{smem + lv * padded_len<P::N>(), 1, 0};
   auto st = op.init(plane, active ? line : 0);
+  typename Op::Acc acc{};
   float2 v[RMAX];
   if (active) {
 #pragma unroll
@@ -136,12 +137,11 @@ __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __
   if constexpr (Op::kStages == 2) {
     if (active) {
 #pragma unroll
-      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q]);
+      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q], acc);
     }
     relayout_out_to_in<P>(v, t, s, BlockSync{});
     fft_run<P, Op::kInv2>(v, t, s, tw, BlockSync{});
   }
-  typename Op::Acc acc{};
   if (active) {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) op.store(st, out_elem<P>(t, q), v[q], acc);
@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __
   const bool active = line < ncols;
   SmemVec s{smem, C, c};
   auto st = op.init(plane, active ? line : 0);
+  typename Op::Acc acc{};
   float2 v[RMAX];
   if (active) {
 #pragma unroll
@@ -175,12 +176,11 @@ __global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __
   if constexpr (Op::kStages == 2) {
     if (active) {
 #pragma unroll
-      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q]);
+      for (int q = 0; q < RMAX; ++q) op.mid(st, out_elem<P>(t, q), v[q], acc);
     }
     relayout_out_to_in<P>(v, t, s, BlockSync{});
     fft_run<P, Op::kInv2>(v, t, s, tw, BlockSync{});
   }
-  typename Op::Acc acc{};
   if (active) {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) op.store(st, out_elem<P>(t, q), v[q], acc);

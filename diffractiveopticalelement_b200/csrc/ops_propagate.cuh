@@ -44,7 +44,7 @@ struct RowF64In : NoReduce {
     const int xs = (x + rx) & (nx - 1);
     return make_float2((float)s.re[xs], (float)s.im[xs]);
   }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.w[x] = v; }
 };
 
@@ -67,7 +67,7 @@ struct RowC64 : NoReduce {
     return {in + p * in_plane_stride + (long)y * nx, out + p * out_plane_stride + (long)y * nx};
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.in[x]; }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.out[x] = cscale(v, scale); }
 };
 
@@ -90,7 +90,7 @@ struct ColC64 : NoReduce {
     return {in + p * in_plane_stride + x, out + p * out_plane_stride + x};
   }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.in[(long)y * nx]; }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const {
     s.out[(long)y * nx] = cscale(v, scale);
   }
@@ -117,7 +117,7 @@ struct ColToF64 : NoReduce {
     return {w + o, re + o, im + o};
   }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.w[(long)y * nx]; }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const {
     s.re[(long)y * nx] = (double)(v.x * scale);
     s.im[(long)y * nx] = (double)(v.y * scale);
@@ -143,7 +143,7 @@ struct ColAsm : NoReduce {
     return {in + o, out + o, asm_col(tab, nx, ny, p, x)};
   }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.in[(long)y * nx]; }
-  __device__ __forceinline__ void mid(const State& s, int y, float2& v) const { v = cmul(v, asm_h_col(s.h, tab, y)); }
+  __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc&) const { v = cmul(v, asm_h_col(s.h, tab, y)); }
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const { s.out[(long)y * nx] = v; }
 };
 
@@ -168,7 +168,7 @@ struct ColSweep : NoReduce {
   __device__ __forceinline__ float2 load(const State& s, int y) const {
     return cmul(s.spec[(long)y * nx], asm_h_col(s.h, tab, y));
   }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const { s.out[(long)y * nx] = v; }
 };
 
@@ -193,7 +193,7 @@ struct RowInvToF64 : NoReduce {
     return {w + p * (long)nx * ny + (long)y * nx, re + o, im + o};
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const {
     s.re[x] = (double)(v.x * scale);
     s.im[x] = (double)(v.y * scale);
@@ -226,7 +226,7 @@ struct ColFocal : NoReduce {
     return {w + o + x, re + o + i, im + o + i, cx[i]};
   }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.w[(long)y * nx]; }
-  __device__ __forceinline__ void mid(const State&, int, float2&) const {}
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const {
     const int j = (y + (ny >> 1)) & (ny - 1);
     float c = s.cxi + cy[j] - 0.25f;

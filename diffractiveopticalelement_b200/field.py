@@ -88,3 +88,54 @@ class ComplexField:
 
     def __repr__(self) -> str:
         return f"ComplexField({self.nx}x{self.ny} @ {self.dx * 1e6:.3f}um)"
+
+
+# ------------------------------------------------------------------ masks (host set-up)
+def _grid(nx, ny, dx, dy):
+    x = (np.arange(nx) - nx / 2) * dx
+    y = (np.arange(ny) - ny / 2) * dy
+    return np.meshgrid(x, y)
+
+
+def discMask(nx, ny, dx, dy, radius, soft=0.0, cx=0.0, cy=0.0):
+    """Disc aperture with optional raised-cosine edge (src/field.js:516-536)."""
+    X, Y = _grid(nx, ny, dx, dy)
+    r = np.hypot(X - cx, Y - cy).ravel()
+    if soft > 0:
+        v = 0.5 * (1 + np.cos((np.pi * (r - radius + soft)) / soft))
+        v = np.where(r <= radius - soft, 1.0, np.where(r >= radius, 0.0, v))
+    else:
+        v = (r <= radius).astype(np.float64)
+    return v
+
+
+def _edge(x, half, soft):
+    v = 0.5 * (1 + np.cos((np.pi * (x - half + soft)) / soft))
+    return np.where(x <= half - soft, 1.0, np.where(x >= half, 0.0, v))
+
+
+def rectMask(nx, ny, dx, dy, width, height, soft=0.0):
+    """Rectangular aperture with optional raised-cosine edge (src/field.js:539-558)."""
+    X, Y = _grid(nx, ny, dx, dy)
+    ax, ay = np.abs(X), np.abs(Y)
+    if soft > 0:
+        fx, fy = _edge(ax, width / 2, soft), _edge(ay, height / 2, soft)
+    else:
+        fx, fy = (ax <= width / 2).astype(np.float64), (ay <= height / 2).astype(np.float64)
+    return (fx * fy).ravel()
+
+
+def ringMask(nx, ny, inner=0.5, outer=0.95, soft=0.02):
+    """Annulus in half-window units (src/doe.js:288-305)."""
+    v = (np.arange(ny) - ny / 2) / (ny / 2)
+    u = (np.arange(nx) - nx / 2) / (nx / 2)
+    U, V = np.meshgrid(u, v)
+    r = np.hypot(U, V).ravel()
+    lo, hi = inner + soft, outer - soft
+    out = np.zeros_like(r)
+    out[(r >= lo) & (r <= hi)] = 1.0
+    m = (r > inner) & (r < lo)
+    out[m] = 0.5 * (1 - np.cos((np.pi * (r[m] - inner)) / soft))
+    m = (r > hi) & (r < outer)
+    out[m] = 0.5 * (1 + np.cos((np.pi * (r[m] - hi)) / soft))
+    return out

@@ -122,6 +122,88 @@ int doe_asm_sweep_dev(doe_ctx* ctx, const void* d_fields, int nfields, int nx, i
                       double dx, double dy, const double* lambda, const double* z, int nz,
                       int band_limit, int evanescent, double soft_edge, void* d_out);
 
+/* ------------------------------------------------------------ design loops */
+typedef enum doe_algorithm {
+  DOE_ALG_GS = 0,          /* gerchbergSaxton (HIO when feedback > 0) -- src/doe.js:327-437 */
+  DOE_ALG_WGS = 1,         /* weightedGerchbergSaxton over gerchbergSaxton -- src/doe.js:455-546 */
+  DOE_ALG_FOURIER = 2,     /* fourierCgh -- src/doe.js:639-730 */
+  DOE_ALG_WGS_FOURIER = 3  /* weightedGerchbergSaxton over fourierCgh -- src/doe.js:898-905 */
+} doe_algorithm;
+
+/* One design; planes are nx*ny FP64 arrays in the reference's layout. Option
+ * meanings follow src/doe.js:49-59 and :327-335. roi, init_phase may be NULL
+ * (NULL init_phase: flat for GS/WGS, randomPhase(seed) for the Fourier loop). */
+typedef struct doe_design_desc {
+  int nx, ny;
+  double dx, dy, lambda, z;
+  int algorithm;
+  int iterations;
+  double feedback; /* HIO feedback, 0 = plain GS */
+  int escape;      /* iterations before the feedback applies */
+  double beta;     /* WGS exponent */
+  double seed;
+  const double* illumination;
+  const double* target_amp; /* target amplitude (already power-matched, src/doe.js:817-829) */
+  const double* roi;
+  const double* init_phase;
+} doe_design_desc;
+
+/* Caller-owned outputs: phase/amplitude/intensity/weights nx*ny, error/efficiency
+ * `iterations` entries; any may be NULL except phase. */
+typedef struct doe_design_result {
+  double* phase;
+  double* amplitude;
+  double* intensity;
+  double* error;
+  double* efficiency;
+  double* weights; /* WGS only */
+  double rmse;     /* WGS only: best unweighted ROI RMSE */
+} doe_design_result;
+
+/* randomPhase(nx, ny, seed) -- src/doe.js:81-86 (xorshift32 makeRng, :65-75):
+ * the seeded initial phase in (-pi, pi]. Host-side, needs no context. */
+int doe_random_phase(int nx, int ny, double seed, double* out);
+
+/* gerchbergSaxton / weightedGerchbergSaxton / fourierCgh on one design. */
+int doe_design(doe_ctx* ctx, const doe_design_desc* desc, doe_design_result* result);
+/* n designs sharing grid, pitch, algorithm and iterations, run as one batch. */
+int doe_design_batch(doe_ctx* ctx, int n, const doe_design_desc* desc, doe_design_result* result);
+
+/* Device-resident batch: FP32 planes [batch][nx*ny] in HBM, asynchronous on the
+ * context's stream. lambdas/zs (host, batch entries) may be NULL: lambda/z apply
+ * to all. phase holds the initial phase on entry and the result on return. */
+typedef struct doe_design_dev_desc {
+  int batch, nx, ny;
+  double dx, dy, lambda, z;
+  const double* lambdas;
+  const double* zs;
+  int algorithm, iterations;
+  double feedback;
+  int escape;
+  double beta;
+  const float* illumination;
+  const float* target_amp;
+  const float* roi;  /* may be NULL */
+  float* phase;
+  float* amplitude;  /* may be NULL */
+  float* weights;    /* may be NULL */
+  double* error;     /* [batch][iterations], may be NULL */
+  double* efficiency;
+  double* rmse;      /* [batch], WGS, may be NULL */
+} doe_design_dev_desc;
+int doe_design_dev(doe_ctx* ctx, const doe_design_dev_desc* desc);
+
+/* gerchbergSaxtonMultiPlane -- src/doe.js:557-626. nplanes target planes at
+ * distances z[p] with target_amp / roi planes p*nx*ny (roi may be NULL) and
+ * weights weight[p] (NULL = 1). per_plane_error is nplanes*iterations (row p =
+ * plane p); error and efficiency follow the reference (mean weighted error,
+ * 1 - error). */
+int doe_multiplane(doe_ctx* ctx, int nx, int ny, double dx, double dy, double lambda,
+                   const double* illumination, int nplanes, const double* z,
+                   const double* target_amp, const double* roi, const double* weight,
+                   int iterations, const double* init_phase, double* phase, double* error,
+                   double* efficiency, double* per_plane_error);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. Angular-spectrum propagation of one complex64
  * plane for callers that must not allocate device memory (a host runtime that owns
