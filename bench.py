@@ -164,6 +164,38 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def main_wgs(args, ctx, device, rank, world, local):
+    """--workload wgs256: batched image-plane WGS designs/s as the primary line."""
+    import torch
+    import torch.distributed as dist
+    sampler = ClockSampler(local)
+    steps = max(1, args.steps if args.steps != 20 else 3)
+    sampler.start()
+    r = run_wgs(ctx, device, args.designs, max(args.warmup, 3), steps)
+    clocks = sampler.stop()
+    ms = r["ms_per_step"]
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = args.designs * world / (ms / 1e3)
+    cpu = wgs_cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    if rank == 0:
+        line = {"metric": "256^2 image-plane WGS designs/s (100 iterations, batched)", "value": value,
+                "unit": "designs/s", "n_gpus": world, "steps": steps, "warmup": max(args.warmup, 3),
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "fp32 fields, fp64 reductions", "data": "synthetic",
+                "config": {"workload": "wgs256", "designs": args.designs, "grid": [WGS_N, WGS_N],
+                           "iterations": WGS_ITERS, "pitch_um": 8, "lambda_nm": 532, "z_mm": 30,
+                           "targets": "3-8 seeded rectangles 4-40 px in the central 128^2", "band_limit": False,
+                           "l2_flush": f"{args.designs} designs x 4 MiB of state exceed L2"},
+                "clocks": clocks, "wgs256": r, "cpu_baseline": cpu, "e2e": None,
+                "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def profile_read(E, ctx):
     names = C.create_string_buffer(64 * 64)
     ms = (C.c_double * 64)()
@@ -243,6 +275,116 @@ def run_reference(args, rank, world):
     return 0
 
 
+# ----------------------------------------------------------------- image-plane WGS workload
+WGS_N, WGS_ITERS, WGS_DX, WGS_LAM, WGS_Z = 256, 100, 8e-6, 532e-9, 0.03
+
+
+def wgs_inputs(n_designs, seed0=1):
+    """Seeded 256^2 image-plane WGS designs: rect-apodised square illumination,
+    3-8 random rectangles (4-40 px) inside the central 128^2 window, auto ROI,
+    random initial phase, target power-matched to the illumination."""
+    import diffractiveopticalelement_b200 as E
+    from diffractiveopticalelement_b200.projector import autoRoi, rectangles_target
+    n = WGS_N
+    ill = E.illuminationProfile("rect", n, n, WGS_DX, WGS_DX, {})
+    irr, roi, tgt, ph = [], [], [], []
+    for k in range(n_designs):
+        t = rectangles_target(n, n, seed0 + k)
+        irr.append(t)
+        roi.append(autoRoi(t, n, n))
+        tgt.append(E.prepareTargetAmp(t, ill))
+        ph.append(E.randomPhase(n, n, seed0 + k))
+    return ill, np.array(irr), np.array(roi), np.array(tgt), np.array(ph)
+
+
+def wgs_cpu_baseline(n_designs=None, iters=WGS_ITERS):
+    """Oracle WGS designs on all host threads (one design per thread)."""
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    nd = n_designs or threads
+    ill, irr, roi, tgt, ph = wgs_inputs(nd, seed0=1)
+    idx = [0]
+    lock = threading.Lock()
+
+    def worker():
+        while True:
+            with lock:
+                if idx[0] >= nd:
+                    return
+                k = idx[0]
+                idx[0] += 1
+            O.design("wgs", ill, tgt[k], nx=WGS_N, ny=WGS_N, dx=WGS_DX, lam=WGS_LAM, z=WGS_Z, iterations=iters,
+                     roi=roi[k], init_phase=ph[k])
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    return {"value": nd / dt, "unit": "designs/s", "cores": threads, "kind": "port",
+            "sample": f"{nd} designs of 256^2 WGS x {iters} iterations (one per thread), FP64 C restatement of "
+                      f"weightedGerchbergSaxton (no JS runtime on this box)"}
+
+
+def run_wgs(ctx, device, n_designs, warmup, steps):
+    """Batched image-plane WGS: designs/s, screen RMSE of every design, kernel split."""
+    import torch
+    import diffractiveopticalelement_b200 as E
+    from diffractiveopticalelement_b200 import _lib
+    L = ctx.lib
+    n = WGS_N * WGS_N
+    ill, irr, roi, tgt, ph = wgs_inputs(n_designs)
+    f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
+    d_ill = f32(np.broadcast_to(ill, (n_designs, n)))
+    d_tgt, d_roi, d_irr, d_ph0 = f32(tgt), f32(roi), f32(irr), f32(ph)
+    d_ph = torch.empty_like(d_ph0)
+    d_amp = torch.empty_like(d_ph0)
+    d_err = torch.empty((n_designs, WGS_ITERS), dtype=torch.float64, device=device)
+    d_eff = torch.empty_like(d_err)
+    d_rmse = torch.empty(n_designs, dtype=torch.float64, device=device)
+    d_met = torch.empty((n_designs, 6), dtype=torch.float64, device=device)
+    desc = _lib.DesignDevDesc(n_designs, WGS_N, WGS_N, WGS_DX, WGS_DX, WGS_LAM, WGS_Z, None, None,
+                              _lib.DOE_ALG_WGS, WGS_ITERS, 0.0, 0, 0.9, d_ill.data_ptr(), d_tgt.data_ptr(),
+                              d_roi.data_ptr(), d_ph.data_ptr(), d_amp.data_ptr(), None, d_err.data_ptr(),
+                              d_eff.data_ptr(), d_rmse.data_ptr())
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+
+    def step():
+        with torch.cuda.stream(stream):
+            d_ph.copy_(d_ph0)  # the initial phase is an input of every design
+        ctx.check(L.doe_design_dev(ctx.h, C.byref(desc)))
+        ctx.check(L.doe_screen_metrics_dev(ctx.h, n_designs, WGS_N, WGS_N, d_amp.data_ptr(), d_irr.data_ptr(), n,
+                                           d_roi.data_ptr(), d_ill.data_ptr(), n, WGS_DX, WGS_DX, WGS_DX, WGS_DX,
+                                           d_met.data_ptr()))
+
+    for _ in range(warmup):
+        step()
+    ctx.synchronize()
+    n0 = L.doe_ctx_launch_count(ctx.h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = int(L.doe_ctx_launch_count(ctx.h) - n0)
+    L.doe_ctx_set_profiling(ctx.h, 1)
+    step()
+    prof = profile_read(None, ctx)
+    L.doe_ctx_set_profiling(ctx.h, 0)
+    met = d_met.cpu().numpy()
+    rm = met[:, 0]
+    return {"designs": n_designs, "iterations": WGS_ITERS, "ms_per_step": ms, "designs_per_s": n_designs / (ms / 1e3),
+            "screen_rmse": {"median": float(np.median(rm)), "min": float(rm.min()), "max": float(rm.max()),
+                            "le_1pct": int(np.sum(rm <= 0.01))},
+            "efficiency_median": float(np.median(met[:, 1])), "gpu_launches_per_step": launches / steps,
+            "per_kernel_ms": {k: round(v[0], 3) for k, v in prof.items()}}
+
+
 # ----------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -253,6 +395,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-fields", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "wgs256"])
+    ap.add_argument("--designs", type=int, default=1024, help="designs per step of the WGS workload")
+    ap.add_argument("--no-wgs", action="store_true", help="skip the WGS block of the default line")
     ap.add_argument("--fields", type=int, default=NFIELDS,
                     help="fields per step (profiling runs use fewer; the benchmark uses 64)")
     args = ap.parse_args()
@@ -278,9 +423,8 @@ def main():
     import diffractiveopticalelement_b200 as E
     ctx = E.Context(local)
     L = ctx.lib
-    L.doe_ctx_launch_count.restype = C.c_ulonglong
-    L.doe_ctx_launch_count.argtypes = [C.c_void_p]
-    L.doe_ctx_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    if args.workload == "wgs256":
+        return main_wgs(args, ctx, device, rank, world, local)
 
     params = workload_params(seed=2024 + rank)[:max(1, min(args.fields, NFIELDS))]
     nfields = len(params)
@@ -405,12 +549,21 @@ def main():
                "sample": f"{nplanes} band-limited 1024^2 propagations of the workload (fields 0-3) on {threads} "
                          f"threads, FP64 C restatement of propagateAngularSpectrum (no JS runtime on this box)"}
 
+    wgs = None
+    if rank == 0 and not args.no_wgs:
+        del out
+        out = None
+        torch.cuda.empty_cache()
+        wgs = run_wgs(ctx, device, min(args.designs, 512), 1, 2)
+        wgs["note"] = ("secondary workload (256^2 image-plane WGS, 100 iterations, seeded rectangle targets); "
+                       "bench.py --workload wgs256 makes it the primary line")
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32), fp64 phase reduction",
                 "data": "synthetic", "config": dict(CONFIG, fields=nfields, tuned_variants=tuned), "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches}
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "wgs256": wgs}
         print(json.dumps(line), flush=True)
     del out, fields
     ctx.close()

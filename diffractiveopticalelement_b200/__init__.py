@@ -11,6 +11,7 @@ from .field import ComplexField, discMask, rectMask, ringMask
 from .doe import (DEFAULT_DESIGN, blurRaster, designDOE, flatPhase, fourierCgh, gerchbergSaxton,
                   gerchbergSaxtonMultiPlane, illuminationProfile, kinoformLens, makeRng, prepareTargetAmp,
                   randomPhase, weightedGerchbergSaxton, wrapPhase)
+from .projector import DEFAULT_PROJECTOR, ProjectorSystem, autoRoi, makeTarget
 from .propagate import (
     DEFAULT_WAVELENGTH,
     angularSpectrumTransferFunction,
@@ -31,4 +32,5 @@ __all__ = [
     "propagateAngularSpectrumInPlace", "discMask", "rectMask", "ringMask", "DEFAULT_DESIGN", "blurRaster",
     "designDOE", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
     "kinoformLens", "makeRng", "prepareTargetAmp", "randomPhase", "weightedGerchbergSaxton", "wrapPhase",
+    "DEFAULT_PROJECTOR", "ProjectorSystem", "autoRoi", "makeTarget",
 ]

@@ -92,6 +92,10 @@ def _declare(L):
         "doe_asm_c64_noalloc": (i, [_vp, _vp, i, i, d, d, d, d, i, i, d, _vp, C.c_char_p, i]),
         "doe_design": (i, [ctxp, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_random_phase": (i, [i, i, d, _dp]),
+        "doe_simulate": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, i, i, i, _dp, _dp, _dp]),
+        "doe_screen_metrics": (i, [ctxp, _dp, _dp, i, i, d, d, _dp, _dp, _dp, d, d, _dp]),
+        "doe_screen_metrics_dev": (i, [ctxp, i, i, i, _vp, _vp, C.c_longlong, _vp, _vp, C.c_longlong, d, d, d, d,
+                                       _vp]),
         "doe_design_batch": (i, [ctxp, i, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
         "doe_multiplane": (i, [ctxp, i, i, d, d, d, _dp, i, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]),

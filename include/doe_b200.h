@@ -204,6 +204,32 @@ int doe_multiplane(doe_ctx* ctx, int nx, int ny, double dx, double dy, double la
                    int iterations, const double* init_phase, double* phase, double* error,
                    double* efficiency, double* per_plane_error);
 
+/* ------------------------------------------------------------ projector */
+/* ProjectorSystem.simulate -- src/projector.js:475-498: the element A exp(i phi)
+ * (illumination, phase: nx*ny FP64) is formed on the device, zero-padded to
+ * pad*nx x pad*ny (image plane, src/field.js:443-461), propagated by the angular
+ * spectrum to z (band_limit as given), centre-cropped; far_field instead applies
+ * focalPlaneSpectrum with f = z. out_d receives the screen pitch. */
+int doe_simulate(doe_ctx* ctx, const double* illumination, const double* phase, int nx, int ny,
+                 double dx, double dy, double lambda, double z, int band_limit, int far_field,
+                 int pad, double* out_re, double* out_im, double* out_d);
+
+/* ProjectorSystem.screenMetrics, radiometric subset -- src/projector.js:554-595
+ * with src/metrics.js:10-18, :73-84: out = {rmse, efficiency, fluxFraction,
+ * powerInSignal, powerAtScreen, powerIncident}. roi may be NULL. */
+int doe_screen_metrics(doe_ctx* ctx, const double* re, const double* im, int nx, int ny,
+                       double sdx, double sdy, const double* target_irr, const double* roi,
+                       const double* illumination, double dx, double dy, double* out);
+
+/* Batched screen metrics of B device-resident screens given by their amplitudes
+ * (FP32 [B][nx*ny]); target/roi/illumination use the given design strides (0 =
+ * shared). out is a device array [B][6] in the order of doe_screen_metrics.
+ * Asynchronous on the context's stream. */
+int doe_screen_metrics_dev(doe_ctx* ctx, int batch, int nx, int ny, const float* amplitude,
+                           const float* target_irr, long long target_stride, const float* roi,
+                           const float* illumination, long long illumination_stride, double sdx,
+                           double sdy, double dx, double dy, double* out);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. Angular-spectrum propagation of one complex64
  * plane for callers that must not allocate device memory (a host runtime that owns
