@@ -127,14 +127,14 @@ struct ColFourier {
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.W[(long)y * b.nx]; }
   __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc& acc) const {
     const long j = (long)rotn(y, b.ny) * b.nx;
+    const float m = s.m ? __ldg(&s.m[j]) : 1.f;
+    const float t0 = __ldg(&s.t[j]);
+    float w = 1.f;
+    if constexpr (WGS) w = s.w[j] * s.wn;
     v = cscale(v, norm);
     const float a = sqrtf(v.x * v.x + v.y * v.y);
     const double ad = a;
     s.amp[j] = a;
-    const float m = s.m ? s.m[j] : 1.f;
-    const float t0 = s.t[j];
-    float w = 1.f;
-    if constexpr (WGS) w = s.w[j] * s.wn;
     const float tw = t0 * w;
     acc.v[kTotal] += ad * ad;
     if (m > 0.f) {
@@ -207,9 +207,9 @@ struct RowDoeFwd : NoReduce {
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const {
     const int xs = ROT ? rotn(x, b.nx) : x;
+    const float a = __ldg(&s.A[xs]);
     float sn, cs;
-    sincosf(s.ph[xs], &sn, &cs);
-    const float a = s.A[xs];
+    sincosf(__ldg(&s.ph[xs]), &sn, &cs);
     return make_float2(a * cs, a * sn);
   }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
@@ -250,16 +250,17 @@ struct RowDoeUpdate : NoReduce {
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
   __device__ __forceinline__ float2 doe(const State& s, int x, float2 v) const {
     const int xi = ROT ? rotn(x, b.nx) : x;
+    const float a = __ldg(&s.A[xi]);
     const float ph = atan2f(v.y, v.x);
-    s.ph[xi] = ph;
     if constexpr (SNAP) {
       if (s.snap) {
+        const float am = s.amp[xi];
         s.bph[xi] = ph;
-        s.bamp[xi] = s.amp[xi];
+        s.bamp[xi] = am;
       }
     }
+    s.ph[xi] = ph;
     const float2 u = unit_phasor(v);
-    const float a = s.A[xi];
     return make_float2(a * u.x, a * u.y);
   }
   __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc&) const { v = doe(s, x, v); }
@@ -304,8 +305,8 @@ struct RowGsTarget {
   __device__ __forceinline__ float measure(const State& s, int x, float2 u, Acc& acc) const {
     const float a = sqrtf(u.x * u.x + u.y * u.y);
     const double ad = a, i2 = ad * ad;
-    const float m = s.m ? s.m[x] : 1.f;
-    const double t = s.t[x];
+    const float m = s.m ? __ldg(&s.m[x]) : 1.f;
+    const double t = __ldg(&s.t[x]);
     acc.v[kTotal] += i2;
     if (m > 0.f) {
       acc.v[kInRoi] += i2 * m;
@@ -324,8 +325,8 @@ struct RowGsTarget {
   __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc& acc) const {
     const float2 u = cscale(v, scale);
     const float a = measure(s, x, u, acc);
-    const float m = s.m ? s.m[x] : 1.f;
-    const float t = s.t[x];
+    const float m = s.m ? __ldg(&s.m[x]) : 1.f;
+    const float t = __ldg(&s.t[x]);
     float na;
     if (m > 0.f) {
       na = t;
@@ -390,21 +391,23 @@ struct RowWgsTarget {
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.W[x]; }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc& acc) const {
+    const float m = s.m ? __ldg(&s.m[x]) : 1.f;
+    const float t = __ldg(&s.t[x]);
+    float wold = 0.f;
+    if constexpr (!INITIAL) wold = s.w[x];
     const float2 u = cscale(v, scale);
     s.U[x] = u;
     const float a = sqrtf(u.x * u.x + u.y * u.y);
     const double ad = a, i2 = ad * ad;
-    const float m = s.m ? s.m[x] : 1.f;
     acc.v[kTotal] += i2;
     if (m > 0.f) acc.v[kInRoi] += i2 * m;
     if constexpr (!INITIAL) {
       if (m > 0.f) {
-        const float t = s.t[x];
         const double d = ad - (double)t;
         acc.v[kRmseNum] += d * d;
         acc.v[kRmseDen] += (double)t * t;
         const float ratio = a > 1e-30f ? t / a : 2.f;
-        float w = s.w[x] * s.wn * powf(fminf(fmaxf(ratio, 0.25f), 4.f), b.beta);
+        float w = wold * s.wn * powf(fminf(fmaxf(ratio, 0.25f), 4.f), b.beta);
         w = fminf(fmaxf(w, 1e-4f), 1e4f);
         s.w[x] = w;
         acc.v[kWsum] += (double)w * w * t * t;
@@ -464,14 +467,17 @@ struct RowWgsConstrain : NoReduce {
             b.best_phase + o, b.best_amp + o, (float)b.st[p].norm, snap};
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const {
-    const float2 u = s.U[x];
+    const float2 u = __ldg(&s.U[x]);
+    const float m = s.m ? __ldg(&s.m[x]) : 1.f;
+    const float t = __ldg(&s.t[x]);
+    const float w = __ldg(&s.w[x]);
     const float a = sqrtf(u.x * u.x + u.y * u.y);
     if (s.snap) {
-      s.bph[x] = s.ph[x];
+      const float ph = __ldg(&s.ph[x]);
+      s.bph[x] = ph;
       s.bamp[x] = a;
     }
-    const float m = s.m ? s.m[x] : 1.f;
-    if (m > 0.f && a > 0.f) return cscale(u, (s.t[x] * (s.w[x] * s.wn)) / a);
+    if (m > 0.f && a > 0.f) return cscale(u, (t * (w * s.wn)) / a);
     return u;
   }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
