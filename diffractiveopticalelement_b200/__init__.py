@@ -22,6 +22,9 @@ from .propagate import (
     propagate,
     propagateAngularSpectrum,
     propagateAngularSpectrumInPlace,
+    propagateFraunhofer,
+    propagateFresnelFFT,
+    propagateFresnelFFTInverse,
 )
 
 __all__ = [
@@ -29,7 +32,8 @@ __all__ = [
     "fft2d", "fft2dOut", "isPow2", "nextPow2", "ComplexField",
     "DEFAULT_WAVELENGTH", "angularSpectrumTransferFunction", "focalPlaneSpectrum", "focusSweep",
     "fresnelMinDistance", "localFrequencyLimit", "propagate", "propagateAngularSpectrum",
-    "propagateAngularSpectrumInPlace", "discMask", "rectMask", "ringMask", "DEFAULT_DESIGN", "blurRaster",
+    "propagateAngularSpectrumInPlace", "propagateFraunhofer", "propagateFresnelFFT", "propagateFresnelFFTInverse",
+    "discMask", "rectMask", "ringMask", "DEFAULT_DESIGN", "blurRaster",
     "designDOE", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
     "kinoformLens", "makeRng", "prepareTargetAmp", "randomPhase", "weightedGerchbergSaxton", "wrapPhase",
     "DEFAULT_PROJECTOR", "ProjectorSystem", "autoRoi", "makeTarget",

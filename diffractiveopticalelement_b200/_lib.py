@@ -65,7 +65,18 @@ class DesignDevDesc(C.Structure):
                 ("lambda_", C.c_double), ("z", C.c_double), ("lambdas", _dp), ("zs", _dp),
                 ("algorithm", C.c_int), ("iterations", C.c_int), ("feedback", C.c_double), ("escape", C.c_int),
                 ("beta", C.c_double), ("illumination", _vp), ("target_amp", _vp), ("roi", _vp), ("phase", _vp),
-                ("amplitude", _vp), ("weights", _vp), ("error", _vp), ("efficiency", _vp), ("rmse", _vp)]
+                ("amplitude", _vp), ("weights", _vp), ("error", _vp), ("efficiency", _vp), ("rmse", _vp),
+                ("rmse_goal", C.c_double), ("screen_irr", _vp), ("iterations_used", _vp)]
+
+
+class MultiplaneDevDesc(C.Structure):
+    """doe_multiplane_dev_desc (device-resident FP32 planes)."""
+    _fields_ = [("batch", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("lambda_", C.c_double), ("nplanes", C.c_int), ("z", _dp), ("weight", _dp), ("iterations", C.c_int),
+                ("illumination", _vp), ("target_amp", _vp), ("roi", _vp), ("phase", _vp), ("error", _vp),
+                ("efficiency", _vp), ("per_plane_error", _vp)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -87,6 +98,8 @@ def _declare(L):
         "doe_asm": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, i, i, d]),
         "doe_asm_sweep": (i, [ctxp, _dp, _dp, i, i, d, d, d, _dp, i, i, i, d, _dp, _dp]),
         "doe_focal_plane": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, _dp, _dp, _dp]),
+        "doe_fresnel": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, _dp, _dp, _dp]),
+        "doe_fresnel_inverse": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, d, d, _dp, _dp]),
         "doe_fft2d_dev": (i, [ctxp, _vp, i, i, i, i]),
         "doe_asm_sweep_dev": (i, [ctxp, _vp, i, i, i, d, d, _dp, _dp, i, i, i, d, _vp]),
         "doe_asm_c64_noalloc": (i, [_vp, _vp, i, i, d, d, d, d, i, i, d, _vp, C.c_char_p, i]),
@@ -98,6 +111,7 @@ def _declare(L):
                                        _vp]),
         "doe_design_batch": (i, [ctxp, i, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
+        "doe_multiplane_dev": (i, [ctxp, C.POINTER(MultiplaneDevDesc)]),
         "doe_multiplane": (i, [ctxp, i, i, d, d, d, _dp, i, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]),
         "doe_autotune": (i, [ctxp, i, i, d, d, d, d, C.POINTER(C.c_int)]),
         "doe_ctx_set_tuning": (i, [ctxp, C.c_char_p, C.c_longlong]),

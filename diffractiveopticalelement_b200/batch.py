@@ -1,0 +1,169 @@
+"""Batched, device-resident design calls (no reference counterpart).
+
+The reference designs one element per call on host planes (src/doe.js:327-546).
+These wrappers run B designs of one grid size through one engine call on CUDA
+tensors that stay on the device: `design_batch` drives doe_design_dev and
+`multiplane_batch` drives doe_multiplane_dev and `screen_metrics_batch` drives
+doe_screen_metrics_dev. Tensors are float32,
+C-contiguous, shaped [B, ny*nx] (or [ny*nx] for a plane shared by every design
+where noted). Work is ordered against torch's current stream on entry and exit.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+_ALG = {"gs": _lib.DOE_ALG_GS, "wgs": _lib.DOE_ALG_WGS, "fourier": _lib.DOE_ALG_FOURIER,
+        "wgs-fourier": _lib.DOE_ALG_WGS_FOURIER}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _plane(t, B, n, name, shared_ok=False):
+    torch = _torch()
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name}: expected a CUDA tensor")
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise TypeError(f"{name}: expected contiguous float32")
+    if t.numel() == n and shared_ok and B > 1:
+        return t.reshape(1, n).expand(B, n).contiguous()
+    if t.numel() != B * n:
+        raise ValueError(f"{name}: expected {B}x{n} values, got {t.numel()}")
+    return t
+
+
+class _Ordered:
+    """Run engine work on the context stream, ordered after / before torch's stream."""
+
+    def __init__(self, ctx):
+        torch = _torch()
+        self.cur = torch.cuda.current_stream()
+        self.ext = torch.cuda.ExternalStream(ctx.stream, device=self.cur.device)
+
+    def __enter__(self):
+        self.ext.wait_stream(self.cur)
+        return self
+
+    def __exit__(self, *exc):
+        self.cur.wait_stream(self.ext)
+        return False
+
+
+def design_batch(ctx, illumination, target_amp, phase, *, nx, ny, dx, dy=None, lam=532e-9, z=0.03,
+                 iterations=100, algorithm="wgs", beta=0.9, feedback=0.0, escape=0, roi=None,
+                 lambdas=None, zs=None, rmse_goal=0.0, screen_irr=None, history=True):
+    """B designs of one grid in one call (doe_design_dev).
+
+    `phase` holds the initial phases and receives the results (best iterate for
+    WGS). `illumination` may be one shared plane. With rmse_goal > 0 (image-plane
+    WGS) a design stops at the first iteration whose screen RMSE is <= rmse_goal
+    and `iterations_used` says when. Returns a dict of device tensors.
+    """
+    torch = _torch()
+    if algorithm not in _ALG:
+        raise ValueError(f"unknown algorithm {algorithm!r}")
+    n = nx * ny
+    if phase.dim() == 1:
+        raise ValueError("phase: expected [B, n]")
+    B = phase.shape[0]
+    ph = _plane(phase, B, n, "phase")
+    ill = _plane(illumination, B, n, "illumination", shared_ok=True)
+    tgt = _plane(target_amp, B, n, "target_amp")
+    ro = _plane(roi, B, n, "roi")
+    sirr = _plane(screen_irr, B, n, "screen_irr")
+    dev = ph.device
+    amp = torch.empty((B, n), dtype=torch.float32, device=dev)
+    it_h = max(int(iterations), 1)
+    err = torch.empty((B, it_h), dtype=torch.float64, device=dev) if history else None
+    eff = torch.empty((B, it_h), dtype=torch.float64, device=dev) if history else None
+    wgs = algorithm.startswith("wgs")
+    rmse = torch.empty(B, dtype=torch.float64, device=dev) if wgs else None
+    used = torch.empty(B, dtype=torch.int32, device=dev)
+    lam_a = None if lambdas is None else np.ascontiguousarray(lambdas, dtype=np.float64)
+    z_a = None if zs is None else np.ascontiguousarray(zs, dtype=np.float64)
+    for a, nm in ((lam_a, "lambdas"), (z_a, "zs")):
+        if a is not None and a.size != B:
+            raise ValueError(f"{nm}: expected {B} entries")
+    ptr = lambda t: None if t is None else t.data_ptr()
+    desc = _lib.DesignDevDesc(B, nx, ny, dx, dx if dy is None else dy, lam, z, _lib.dp(lam_a), _lib.dp(z_a),
+                              _ALG[algorithm], int(iterations), float(feedback), int(escape), float(beta),
+                              ptr(ill), ptr(tgt), ptr(ro), ptr(ph), ptr(amp), None, ptr(err), ptr(eff), ptr(rmse),
+                              float(rmse_goal), ptr(sirr), ptr(used) if algorithm == "wgs" else None)
+    with _Ordered(ctx):
+        ctx.check(ctx.lib.doe_design_dev(ctx.h, C.byref(desc)))
+    out = {"phase": ph, "amplitude": amp, "error": err, "efficiency": eff}
+    if wgs:
+        out["rmse"] = rmse
+    if algorithm == "wgs":
+        out["iterations_used"] = used
+    return out
+
+
+def screen_metrics_batch(ctx, amplitude, target_irr, illumination, *, nx, ny, sdx, sdy=None, dx=None, dy=None,
+                         roi=None):
+    """Radiometric screen metrics of B screens given by amplitude (doe_screen_metrics_dev).
+
+    Returns a [B, 6] float64 tensor: rmse, efficiency, fluxFraction, powerInSignal,
+    powerAtScreen, powerIncident (src/projector.js:554-595). target_irr, roi and
+    illumination may be single shared planes.
+    """
+    torch = _torch()
+    n = nx * ny
+    B = amplitude.shape[0]
+    amp = _plane(amplitude, B, n, "amplitude")
+    tgt = _plane(target_irr, 1 if target_irr.numel() == n else B, n, "target_irr")
+    ill = _plane(illumination, 1 if illumination.numel() == n else B, n, "illumination")
+    ro = None if roi is None else _plane(roi, 1 if roi.numel() == n else B, n, "roi")
+    if ro is not None and ro.numel() != tgt.numel():
+        raise ValueError("roi and target_irr must both be shared or both per design")
+    out = torch.empty((B, 6), dtype=torch.float64, device=amp.device)
+    sdy = sdx if sdy is None else sdy
+    dx = sdx if dx is None else dx
+    dy = dx if dy is None else dy
+    with _Ordered(ctx):
+        ctx.check(ctx.lib.doe_screen_metrics_dev(ctx.h, B, nx, ny, amp.data_ptr(), tgt.data_ptr(),
+                                                 0 if tgt.numel() == n else n, None if ro is None else ro.data_ptr(),
+                                                 ill.data_ptr(), 0 if ill.numel() == n else n, sdx, sdy, dx, dy,
+                                                 out.data_ptr()))
+    return out
+
+
+def multiplane_batch(ctx, illumination, target_amp, phase, zs, *, nx, ny, dx, dy=None, lam=532e-9, iterations=60,
+                     roi=None, weights=None, history=True):
+    """B multi-plane designs (src/doe.js:557-626) in one call (doe_multiplane_dev).
+
+    target_amp and roi are [B, P, n] (P = len(zs)); `phase` holds the initial
+    phases [B, n] and receives the results. Returns error / efficiency [B, I] and
+    per-plane errors [B, P, I] as device tensors.
+    """
+    torch = _torch()
+    n = nx * ny
+    B = phase.shape[0]
+    P = len(zs)
+    ph = _plane(phase, B, n, "phase")
+    ill = _plane(illumination, B, n, "illumination", shared_ok=True)
+    tgt = _plane(target_amp, B * P, n, "target_amp")
+    ro = _plane(roi, B * P, n, "roi")
+    z_a = np.ascontiguousarray(zs, dtype=np.float64)
+    w_a = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    if w_a is not None and w_a.size != P:
+        raise ValueError(f"weights: expected {P} entries")
+    it_h = max(int(iterations), 1)
+    dev = ph.device
+    err = torch.empty((B, it_h), dtype=torch.float64, device=dev) if history else None
+    eff = torch.empty((B, it_h), dtype=torch.float64, device=dev) if history else None
+    ppe = torch.empty((B, P, it_h), dtype=torch.float64, device=dev) if history else None
+    ptr = lambda t: None if t is None else t.data_ptr()
+    desc = _lib.MultiplaneDevDesc(B, nx, ny, dx, dx if dy is None else dy, lam, P, _lib.dp(z_a), _lib.dp(w_a),
+                                  int(iterations), ptr(ill), ptr(tgt), ptr(ro), ptr(ph), ptr(err), ptr(eff), ptr(ppe))
+    with _Ordered(ctx):
+        ctx.check(ctx.lib.doe_multiplane_dev(ctx.h, C.byref(desc)))
+    return {"phase": ph, "error": err, "efficiency": eff, "perPlaneError": ppe}

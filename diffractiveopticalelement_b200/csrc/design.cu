@@ -45,7 +45,10 @@ __global__ void design_init_kernel(DesignBufs b, int B, bool wgs) {
       b.st[d].norm = 1.0;
       b.st[d].best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
       b.st[d].eff_cur = 0.0;
-      b.st[d].pad = 0.0;
+      b.st[d].stop = -1;
+      b.st[d].pad = 0;
+      b.st[d].sT = 0.0;
+      b.st[d].sTT = 0.0;
     }
   }
 }
@@ -59,6 +62,20 @@ __global__ void design_final_snapshot_kernel(DesignBufs b, int B, int it) {
     const float2 u = b.U[i];
     b.best_phase[i] = b.phase[i];
     b.best_amp[i] = sqrtf(u.x * u.x + u.y * u.y);
+  }
+}
+
+// Designs stopped by the screen goal: iterations run, and the histories past the
+// stop repeat its last entry. One thread per design.
+__global__ void design_goal_out_kernel(DesignBufs b, int B, int iters, int* used) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < B; d += gridDim.x * blockDim.x) {
+    const int stop = b.st[d].stop;
+    if (used) used[d] = stop >= 0 ? stop + 1 : iters;
+    if (stop < 0) continue;
+    for (int i = stop + 1; i < iters; ++i) {
+      b.err_hist[(long)d * b.iters + i] = b.err_hist[(long)d * b.iters + stop];
+      b.eff_hist[(long)d * b.iters + i] = b.eff_hist[(long)d * b.iters + stop];
+    }
   }
 }
 
@@ -120,8 +137,8 @@ static int build_htab(doe_ctx* c, int nx, int ny, double dx, double dy, int ntab
 // Carve the design state of B designs (histories `Ih` long) from kSlotDesign2.
 static int carve_state(doe_ctx* c, DesignBufs& b, int B, int Ih, int bpp, int pp_planes) {
   const size_t bytes = 256 * 8 + sizeof(DesignState) * B + sizeof(double) * (size_t)B * Ih * (2 + pp_planes) +
-                       (size_t)B * Ih + sizeof(double) * (size_t)B * bpp * kRedK + sizeof(unsigned) * B +
-                       sizeof(double) * B * kRedK;
+                       (size_t)B * Ih + sizeof(double) * (size_t)B * bpp * kRedKGoal + sizeof(unsigned) * B +
+                       sizeof(double) * B * kRedKGoal;
   void* p2;
   DOE_TRY(ensure_slot(c, kSlotDesign2, bytes, &p2));
   char* q = (char*)p2;
@@ -130,9 +147,9 @@ static int carve_state(doe_ctx* c, DesignBufs& b, int B, int Ih, int bpp, int pp
   if (!b.eff_hist) b.eff_hist = (double*)take(q, sizeof(double) * (size_t)B * Ih);
   b.pp_err = pp_planes ? (double*)take(q, sizeof(double) * (size_t)B * Ih * pp_planes) : nullptr;
   b.improved = (unsigned char*)take(q, (size_t)B * Ih);
-  b.partials = (double*)take(q, sizeof(double) * (size_t)B * bpp * kRedK);
+  b.partials = (double*)take(q, sizeof(double) * (size_t)B * bpp * kRedKGoal);
   b.counters = (unsigned*)take(q, sizeof(unsigned) * B);
-  b.totals = (double*)take(q, sizeof(double) * B * kRedK);
+  b.totals = (double*)take(q, sizeof(double) * B * kRedKGoal);
   DOE_CUDA(c, cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * B, c->stream));
   DOE_CUDA(c, cudaMemsetAsync(b.improved, 0, (size_t)B * Ih, c->stream));
   return DOE_OK;
@@ -153,6 +170,10 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   const bool fourier = alg == DOE_ALG_FOURIER || alg == DOE_ALG_WGS_FOURIER;
   const bool wgs = alg == DOE_ALG_WGS || alg == DOE_ALG_WGS_FOURIER;
   if (wgs && I < 1) return set_err(c, DOE_ERR_BAD_ARG, "weightedGerchbergSaxton: needs at least one iteration");
+  if (a->rmse_goal < 0 || a->rmse_goal != a->rmse_goal)
+    return set_err(c, DOE_ERR_BAD_ARG, "designDOE: rmse_goal must be >= 0");
+  if (a->rmse_goal > 0 && alg != DOE_ALG_WGS)
+    return set_err(c, DOE_ERR_UNSUPPORTED, "designDOE: a screen RMSE goal needs image-plane WGS");
   if (B > 65535) return set_err(c, DOE_ERR_UNSUPPORTED, "designDOE: at most 65535 designs per call");
   const long n = (long)nx * ny;
   const long Bn = (long)B * n;
@@ -192,6 +213,8 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   b.best_amp = wgs ? (float*)take(q1, Bn * sizeof(float)) : nullptr;
   b.err_hist = a->error;
   b.eff_hist = a->efficiency;
+  b.rmse_goal = a->rmse_goal;
+  b.screen_irr = a->screen_irr;
   DOE_TRY(carve_state(c, b, B, Ih, design_bpp(nx, ny), 0));
   {
     LaunchScope ls(c, "design_init");
@@ -211,9 +234,16 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
     DOE_TRY(design_run_gs(c, b, B, I));
   } else if (!fourier) {
     DOE_TRY(design_run_wgs(c, b, B, I));
-    LaunchScope ls(c, "design_snapshot");
-    design_final_snapshot_kernel<<<grid_for(Bn), 256, 0, c->stream>>>(b, B, I - 1);
-    DOE_CUDA(c, cudaGetLastError());
+    {
+      LaunchScope ls(c, "design_snapshot");
+      design_final_snapshot_kernel<<<grid_for(Bn), 256, 0, c->stream>>>(b, B, I - 1);
+      DOE_CUDA(c, cudaGetLastError());
+    }
+    if (b.rmse_goal > 0 || a->iterations_used) {
+      LaunchScope ls(c, "design_goal_out");
+      design_goal_out_kernel<<<(B + 255) / 256, 256, 0, c->stream>>>(b, B, I, a->iterations_used);
+      DOE_CUDA(c, cudaGetLastError());
+    }
   } else {
     DOE_TRY(design_run_fourier(c, b, B, I, wgs));
   }
@@ -435,7 +465,7 @@ extern "C" int doe_multiplane(doe_ctx* c, int nx, int ny, double dx, double dy, 
   }
   std::vector<double> lam(P, lambda);
   DOE_TRY(build_htab(c, nx, ny, dx, dy, P, lam.data(), zs, htab));
-  DOE_TRY(design_run_multiplane(c, b, I, P, htab, f + 2 * n, roi ? f + (long)(2 + P) * n : nullptr));
+  DOE_TRY(design_run_multiplane(c, b, 1, I, P, htab, f + 2 * n, roi ? f + (long)(2 + P) * n : nullptr));
   DOE_TRY(convert_back_launch(c, b.phase, din, n));
   std::vector<double> ppe((size_t)P * Ih);
   DOE_CUDA(c, cudaMemcpyAsync(phase, din, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -451,5 +481,74 @@ extern "C" int doe_multiplane(doe_ctx* c, int nx, int ny, double dx, double dy, 
   if (per_plane_error)
     for (int p = 0; p < P; ++p)
       for (int it = 0; it < I; ++it) per_plane_error[(size_t)p * I + it] = ppe[(size_t)p * Ih + it];
+  return DOE_OK;
+}
+
+// Per-iteration multi-plane error / efficiency of B designs from the per-plane
+// errors (src/doe.js:601, :618-619). One thread per (design, iteration).
+__global__ void multiplane_hist_kernel(const double* ppe, int B, int P, int Ih, int I, const double* w, double* err,
+                                       double* eff, double* ppe_out) {
+  const long total = (long)B * I;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int d = (int)(i / I), it = (int)(i % I);
+    double e = 0;
+    for (int p = 0; p < P; ++p) {
+      const double v = ppe[((long)d * P + p) * Ih + it];
+      e += v * w[p];
+      if (ppe_out) ppe_out[((long)d * P + p) * I + it] = v;
+    }
+    if (err) err[i] = e / P;
+    if (eff) eff[i] = 1 - e / P;
+  }
+}
+
+extern "C" int doe_multiplane_dev(doe_ctx* c, const doe_multiplane_dev_desc* a) {
+  if (!c || !a) return DOE_ERR_BAD_ARG;
+  DOE_TRY(check_design_grid(c, a->nx, a->ny, "gerchbergSaxtonMultiPlane"));
+  const int B = a->batch, nx = a->nx, ny = a->ny, P = a->nplanes, I = a->iterations;
+  if (P <= 0) return set_err(c, DOE_ERR_BAD_ARG, "gerchbergSaxtonMultiPlane: no planes");
+  if (B <= 0 || I < 0 || !a->z || !a->illumination || !a->target_amp || !a->phase)
+    return set_err(c, DOE_ERR_BAD_ARG, "gerchbergSaxtonMultiPlane: bad argument");
+  if (B > 65535) return set_err(c, DOE_ERR_UNSUPPORTED, "gerchbergSaxtonMultiPlane: at most 65535 designs per call");
+  const long n = (long)nx * ny;
+  const int Ih = std::max(I, 1);
+  void* p0;
+  DOE_TRY(ensure_slot(c, kSlotDesign0, (size_t)B * n * sizeof(float2) + (size_t)P * n * sizeof(float2) +
+                                           (size_t)B * n * sizeof(float) + sizeof(double) * (P + 2) + 2048, &p0));
+  char* q0 = (char*)p0;
+  DesignBufs b;
+  memset(&b, 0, sizeof(b));
+  b.nx = nx;
+  b.ny = ny;
+  b.iters = Ih;
+  b.dx = a->dx;
+  b.dy = a->dy;
+  b.illum = a->illumination;
+  b.phase = a->phase;
+  b.tgt_stride = (long)P * n;
+  b.W = (float2*)take(q0, (size_t)B * n * sizeof(float2));
+  float2* htab = (float2*)take(q0, (size_t)P * n * sizeof(float2));
+  b.amp = (float*)take(q0, (size_t)B * n * sizeof(float));
+  double* dw = (double*)take(q0, sizeof(double) * P);
+  b.htab_stride = 0;
+  b.mp_nplanes = P;
+  DOE_TRY(carve_state(c, b, B, Ih, design_bpp(nx, ny), P));
+  {
+    LaunchScope ls(c, "design_init");
+    design_init_kernel<<<1, 256, 0, c->stream>>>(b, B, false);
+    DOE_CUDA(c, cudaGetLastError());
+  }
+  std::vector<double> lam(P, a->lambda), w(P, 1.0);
+  if (a->weight)
+    for (int p = 0; p < P; ++p) w[p] = a->weight[p];
+  DOE_CUDA(c, cudaMemcpyAsync(dw, w.data(), sizeof(double) * P, cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(build_htab(c, nx, ny, a->dx, a->dy, P, lam.data(), a->z, htab));
+  DOE_TRY(design_run_multiplane(c, b, B, I, P, htab, a->target_amp, a->roi));
+  if (I > 0 && (a->error || a->efficiency || a->per_plane_error)) {
+    LaunchScope ls(c, "multiplane_hist");
+    multiplane_hist_kernel<<<grid_for((long)B * I), 256, 0, c->stream>>>(b.pp_err, B, P, Ih, I, dw, a->error,
+                                                                         a->efficiency, a->per_plane_error);
+    DOE_CUDA(c, cudaGetLastError());
+  }
   return DOE_OK;
 }

@@ -18,10 +18,17 @@ struct DesignState {
   double norm;      // WGS: weights = w_raw * norm
   double best;      // WGS: best unweighted ROI RMSE so far
   double eff_cur;   // image-plane WGS: efficiency of the current forward field
-  double pad;
+  int stop;         // -1 running; else the iteration whose field met the screen goal
+  int pad;
+  double sT, sTT;   // screen goal: sum T over the plane, sum T^2 over the ROI (fixed)
 };
 
 enum RedSlot { kErrNum = 0, kErrDen, kInRoi, kTotal, kRmseNum, kRmseDen, kWsum, kTsum, kRedK };
+// Screen-RMSE sums of the stopping goal (src/projector.js:554-595): per iteration
+// sum I m over the plane and sum I^2, I T over the ROI; the target's sum T (plane)
+// and sum T^2 (ROI) are fixed and summed once, by the first pass, in the first two.
+enum GoalSlot { kSIM = kRedK, kSII, kSIT, kRedKGoal };
+constexpr int kST = kSIM, kSTT = kSII;
 using DesignAcc = DAcc<kRedK>;
 
 struct DesignBufs {
@@ -49,13 +56,19 @@ struct DesignBufs {
   double* pp_err;       // multi-plane: [B][nplanes][iters]
   int mp_plane, mp_nplanes;
   unsigned char* improved;  // [B][iters]
-  double* partials;     // [B][max blocks][kRedK]
+  double* partials;     // [B][max blocks][kRedKGoal]
   unsigned* counters;   // [B]
-  double* totals;       // [B][kRedK]
+  double* totals;       // [B][kRedKGoal]
+  double rmse_goal;     // > 0: image-plane WGS stops a design at this screen RMSE
+  const float* screen_irr;  // [B][n] target irradiance of the goal, or null (t^2)
   __device__ __forceinline__ long pe() const { return (long)nx * ny; }
 };
 
 __device__ __forceinline__ int rotn(int i, int n) { return (i + (n >> 1)) & (n - 1); }
+
+// Designs that met the screen goal drop out of every later pass (whole CTAs
+// return before any barrier: the plane index is uniform per CTA).
+__device__ __forceinline__ bool design_stopped(const DesignState* st, int p) { return st && st[p].stop >= 0; }
 
 __device__ __forceinline__ float2 unit_phasor(float2 v) {
   const float r2 = v.x * v.x + v.y * v.y;
@@ -83,6 +96,8 @@ struct ColAsmTab : NoReduce {
   const float2* htab;
   long htab_stride;
   int nx, ny;
+  const DesignState* st;  // null: every design runs
+  __device__ __forceinline__ bool skip(int p) const { return design_stopped(st, p); }
   struct State {
     float2* w;
     const float2* h;
@@ -230,6 +245,7 @@ struct RowDoeUpdate : NoReduce {
   static constexpr bool kInv1 = true, kInv2 = false;
   DesignBufs b;
   int snap_it;  // iteration whose improvement flag is consulted (SNAP)
+  __device__ __forceinline__ bool skip(int p) const { return design_stopped(b.st, p); }
   struct State {
     const float* A;
     float* ph;
@@ -365,28 +381,34 @@ struct RowGsTarget {
 // the weight update (w <- clamp(w clamp(t/a, 1/4, 4)^beta, 1e-4, 1e4), stored
 // before normalisation). The last CTA of a design records the histories, the best
 // RMSE and the new normalisation sqrt(sum t^2 / sum w^2 t^2). INITIAL only
-// measures the efficiency of the first forward field.
-template <bool INITIAL>
+// measures the efficiency of the first forward field. GOAL also sums the screen
+// RMSE of the field (same definition as screen_metrics_kernel) and stops the
+// design when it reaches b.rmse_goal; that iterate is forced into the snapshot.
+template <bool INITIAL, bool GOAL = false>
 struct RowWgsTarget {
   static constexpr const char* kName = INITIAL ? "design_row_wgs_first" : "design_row_wgs_target";
   static constexpr int kStages = 1;
   static constexpr bool kInv1 = true, kInv2 = false;
-  using Acc = DesignAcc;
+  static constexpr int K = GOAL ? kRedKGoal : kRedK;
+  using Acc = DAcc<K>;
   DesignBufs b;
   int it;
   float scale;
+  __device__ __forceinline__ bool skip(int p) const { return design_stopped(b.st, p); }
   struct State {
     const float* t;
     const float* m;
     float* w;
     float2* U;
     const float2* W;
+    const float* T;
     float wn;
   };
   __device__ __forceinline__ State init(int p, int y) const {
     const long o = p * b.pe() + (long)y * b.nx;
     const long ot = p * b.tgt_stride + (long)y * b.nx;
-    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, (float)b.st[p].norm};
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o,
+            (GOAL && b.screen_irr) ? b.screen_irr + o : nullptr, (float)b.st[p].norm};
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.W[x]; }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
@@ -414,18 +436,46 @@ struct RowWgsTarget {
         acc.v[kTsum] += (double)t * t;
       }
     }
+    if constexpr (GOAL) {
+      const double T = s.T ? (double)__ldg(&s.T[x]) : (double)t * t;
+      if constexpr (INITIAL) {
+        acc.v[kST] += T;
+        if (m > 0.f) acc.v[kSTT] += T * T;
+      } else {
+        acc.v[kSIM] += i2 * m;
+        if (m > 0.f) {
+          acc.v[kSII] += i2 * i2;
+          acc.v[kSIT] += i2 * T;
+        }
+      }
+    }
   }
   __device__ __forceinline__ void finish(int p, int bip, int bpp, Acc& acc) const {
-    if (!design_reduce(b, p, bip, bpp, acc) || threadIdx.x != 0) return;
-    const double* T = b.totals + (long)p * kRedK;
+    if (!group_reduce<K>(acc, p, bip, bpp, b.partials, b.counters, b.totals) || threadIdx.x != 0) return;
+    const double* T = b.totals + (long)p * K;
     DesignState& S = b.st[p];
     const double eff = T[kTotal] > 0 ? (T[kInRoi] * b.dx * b.dy) / (T[kTotal] * b.dx * b.dy) : 0.0;
     if constexpr (INITIAL) {
       S.eff_cur = eff;
+      if constexpr (GOAL) {
+        S.sT = T[kST];
+        S.sTT = T[kSTT];
+      }
     } else {
       const long h = (long)p * b.iters + it;
       const double rmse = T[kRmseDen] > 0 ? sqrt(T[kRmseNum] / T[kRmseDen]) : 0.0;
-      const bool imp = rmse < S.best;
+      bool imp = rmse < S.best;
+      if constexpr (GOAL) {
+        // screen RMSE exactly as screen_metrics_kernel (the pitch cancels)
+        const double sc = S.sT > 0 ? T[kSIM] / S.sT : 0.0;
+        const double den = sc * sc * S.sTT;
+        const double num = fmax(0.0, T[kSII] - 2.0 * sc * T[kSIT] + sc * sc * S.sTT);
+        const double srm = den > 0 ? sqrt(num / den) : 0.0;
+        if (srm <= b.rmse_goal) {
+          S.stop = it;
+          imp = true;  // return the iterate that met the goal
+        }
+      }
       if (imp) S.best = rmse;
       b.improved[h] = imp ? 1 : 0;
       b.err_hist[h] = S.best;
@@ -447,6 +497,8 @@ struct RowWgsConstrain : NoReduce {
   static constexpr bool kInv1 = false, kInv2 = false;
   DesignBufs b;
   int snap_it;  // -1: no snapshot check
+  // a stopped design runs this pass once more, for the snapshot of its last iterate
+  __device__ __forceinline__ bool skip(int p) const { return design_stopped(b.st, p) && b.st[p].stop != snap_it; }
   struct State {
     const float* t;
     const float* m;
@@ -534,9 +586,9 @@ inline int design_bpp(int nx, int ny) {
 int design_run_gs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
 int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
 int design_run_fourier(doe_ctx* c, const DesignBufs& b, int B, int iterations, bool wgs);
-// Multi-plane (one design): plane p uses transfer table htab + p*n and target /
-// ROI planes tgt0 + p*n, roi0 + p*n (roi0 may be null).
-int design_run_multiplane(doe_ctx* c, DesignBufs b, int iterations, int nplanes, const float2* htab,
+// Multi-plane (B designs): plane p uses transfer table htab + p*n and target /
+// ROI planes tgt0 + d*nplanes*n + p*n (roi0 may be null).
+int design_run_multiplane(doe_ctx* c, DesignBufs b, int B, int iterations, int nplanes, const float2* htab,
                           const float* tgt0, const float* roi0);
 
 }  // namespace doe

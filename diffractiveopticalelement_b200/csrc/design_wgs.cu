@@ -7,17 +7,25 @@ namespace doe {
 int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int I) {
   const int nx = b.nx, ny = b.ny;
   const float scale = 1.f / (float)((long)nx * ny);
-  const ColAsmTab<false> fwd{{}, b.W, b.htab, b.htab_stride, nx, ny};
-  const ColAsmTab<true> back{{}, b.W, b.htab, b.htab_stride, nx, ny};
+  const ColAsmTab<false> fwd{{}, b.W, b.htab, b.htab_stride, nx, ny, b.st};
+  const ColAsmTab<true> back{{}, b.W, b.htab, b.htab_stride, nx, ny, b.st};
   DOE_TRY(design_row(c, RowDoeFwd<false>{{}, b}, B, nx, ny));
   DOE_TRY(design_col(c, fwd, B, nx, ny));
-  DOE_TRY(design_row(c, RowWgsTarget<true>{b, 0, scale}, B, nx, ny));
+  if (b.rmse_goal > 0) {
+    DOE_TRY(design_row(c, RowWgsTarget<true, true>{b, 0, scale}, B, nx, ny));
+  } else {
+    DOE_TRY(design_row(c, RowWgsTarget<true>{b, 0, scale}, B, nx, ny));
+  }
   for (int it = 0; it < I; ++it) {
     DOE_TRY(design_row(c, RowWgsConstrain{{}, b, it - 1}, B, nx, ny));
     DOE_TRY(design_col(c, back, B, nx, ny));
     DOE_TRY(design_row(c, RowDoeUpdate<true, false, false>{{}, b, 0}, B, nx, ny));
     DOE_TRY(design_col(c, fwd, B, nx, ny));
-    DOE_TRY(design_row(c, RowWgsTarget<false>{b, it, scale}, B, nx, ny));
+    if (b.rmse_goal > 0) {
+      DOE_TRY(design_row(c, RowWgsTarget<false, true>{b, it, scale}, B, nx, ny));
+    } else {
+      DOE_TRY(design_row(c, RowWgsTarget<false>{b, it, scale}, B, nx, ny));
+    }
   }
   return DOE_OK;
 }

@@ -16,6 +16,8 @@
 // is called for inactive lines too (with a clamped line index) and must not fault.
 #pragma once
 #include <tuple>
+#include <type_traits>
+#include <utility>
 
 #include "fft_core.cuh"
 
@@ -107,6 +109,21 @@ struct BlockSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
 
+// Operators may expose `bool skip(int plane)`: a CTA whose plane is skipped
+// returns before its first barrier (the plane is uniform per CTA).
+template <class Op, class = void>
+struct HasSkip : std::false_type {};
+template <class Op>
+struct HasSkip<Op, std::void_t<decltype(std::declval<const Op&>().skip(0))>> : std::true_type {};
+template <class Op>
+__device__ __forceinline__ bool op_skip(const Op& op, int plane) {
+  if constexpr (HasSkip<Op>::value) {
+    return op.skip(plane);
+  } else {
+    return false;
+  }
+}
+
 // Row pass. Grid: nplanes * ceil(nlines / V) CTAs; rows beyond nlines idle.
 template <class S, class Op>
 __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __restrict__ tw, int nlines) {
@@ -122,6 +139,7 @@ __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __
   const int bip = blockIdx.x % bpp;
   const int line = bip * V + lv;
   const bool active = line < nlines;
+  if (op_skip(op, plane)) return;
   SmemVec s{smem + lv * padded_len<P::N>(), 1, 0};
   auto st = op.init(plane, active ? line : 0);
   typename Op::Acc acc{};
@@ -161,6 +179,7 @@ __global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __
   const int plane = blockIdx.y;
   const int line = blockIdx.x * C + c;
   const bool active = line < ncols;
+  if (op_skip(op, plane)) return;
   SmemVec s{smem, C, c};
   auto st = op.init(plane, active ? line : 0);
   typename Op::Acc acc{};

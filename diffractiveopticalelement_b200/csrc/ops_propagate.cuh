@@ -239,6 +239,80 @@ struct ColFocal : NoReduce {
   }
 };
 
+// Single-FFT Fresnel transforms (src/propagate.js:155-316). Both quadratic
+// factors are separable: cycles(x, y) = cx[x] + cy[y], each axis term reduced
+// mod 1 in FP64 on the host with the checkerboard (-1)^(i+j) folded in as half a
+// cycle on odd indices and the sign of the chirp (forward +, inverse -) applied.
+// Row pass: FP64 split planes x chirp, row FFT.
+template <bool INV>
+struct RowChirpIn : NoReduce {
+  static constexpr const char* kName = INV ? "fresnel_row_inv" : "fresnel_row_fwd";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = INV, kInv2 = false;
+  const double* re;
+  const double* im;
+  float2* w;
+  const float* cx;  // [nx] cycles
+  const float* cy;  // [ny]
+  int nx, ny;
+  struct State {
+    const double* re;
+    const double* im;
+    float2* w;
+    float cyj;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * (long)nx * ny + (long)y * nx;
+    return {re + o, im + o, w + o, cy[y]};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const {
+    const float2 u = make_float2((float)s.re[x], (float)s.im[x]);
+    float c = __ldg(&cx[x]) + s.cyj;
+    c -= rintf(c);
+    float sn, cs;
+    sincospif(2.f * c, &sn, &cs);
+    return cmul(u, make_float2(cs, sn));
+  }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.w[x] = v; }
+};
+
+// Column pass: column FFT, x pre (prefactor incl. any 1/N) x output chirp, FP64 out.
+template <bool INV>
+struct ColChirpOut : NoReduce {
+  static constexpr const char* kName = INV ? "fresnel_col_inv" : "fresnel_col_fwd";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = INV, kInv2 = false;
+  const float2* w;
+  double* re;
+  double* im;
+  const float* cu;  // [nx] cycles
+  const float* cv;  // [ny]
+  int nx, ny;
+  float2 pre;
+  struct State {
+    const float2* w;
+    double* re;
+    double* im;
+    float cux;
+  };
+  __device__ __forceinline__ State init(int p, int x) const {
+    const long o = p * (long)nx * ny + x;
+    return {w + o, re + o, im + o, cu[x]};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int y) const { return s.w[(long)y * nx]; }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const {
+    float c = s.cux + __ldg(&cv[y]);
+    c -= rintf(c);
+    float sn, cs;
+    sincospif(2.f * c, &sn, &cs);
+    const float2 z = cmul(cmul(v, pre), make_float2(cs, sn));
+    s.re[(long)y * nx] = (double)z.x;
+    s.im[(long)y * nx] = (double)z.y;
+  }
+};
+
 // Shared entry points implemented in prop_*.cu.
 int fft2d_c64(doe_ctx* c, float2* d, int nx, int ny, int nplanes, bool inverse);
 int asm_c64_inplace(doe_ctx* c, float2* d, int nplanes, const AsmTables& tab, int nx, int ny, float2* work);

@@ -5,7 +5,8 @@ Same names, argument meaning and option defaults as the reference:
 ``propagateAngularSpectrum`` / ``propagateAngularSpectrumInPlace`` (:105-133),
 ``focalPlaneSpectrum`` (:342-374), ``focusSweep`` (:427-434),
 ``localFrequencyLimit`` (:48-51), ``fresnelMinDistance`` (:141-143),
-``propagate`` (:383-389).
+``propagateFresnelFFT`` / ``propagateFraunhofer`` (:155-230, :310-312),
+``propagateFresnelFFTInverse`` (:237-308), ``propagate`` (:383-389).
 """
 from __future__ import annotations
 
@@ -105,15 +106,60 @@ def focusSweep(field: ComplexField, lam, zStart, zEnd, steps, opts=None, *, ctx=
     return planes
 
 
+def propagateFresnelFFT(field: ComplexField, lam, z, opts=None, *, ctx=None, **kw):
+    """Single-FFT Fresnel propagation to the magnified grid (src/propagate.js:155-230).
+
+    Returns {field, dx, dy, z, magnification, undersampled, zCritical} like the
+    reference; throwOnUndersampled raises the reference's error below z_c.
+    """
+    throw = bool(_opt(opts, kw, "throwOnUndersampled", False))
+    nx, ny, dx, dy = field.nx, field.ny, field.dx, field.dy
+    az = abs(z)
+    z_c = fresnelMinDistance(nx, dx, lam)
+    under = az < z_c
+    if under and throw:
+        raise ValueError(
+            f"propagateFresnelFFT: z={az * 1e3:.3f} mm is below the critical distance "
+            f"z_c={z_c * 1e3:.3f} mm for a {nx}x{ny} grid at {dx * 1e6:.2f} um pitch — the Fresnel chirp is "
+            f"under-sampled. Use the angular spectrum instead.")
+    c = ctx or _lib.context()
+    out = ComplexField(nx, ny, 1.0, 1.0)
+    d = np.zeros(2)
+    c.check(c.lib.doe_fresnel(c.h, _lib.dp(field.re), _lib.dp(field.im), nx, ny, dx, dy, float(lam), float(z),
+                              _lib.dp(out.re), _lib.dp(out.im), _lib.dp(d)))
+    out.dx, out.dy = float(d[0]), float(d[1])
+    return {"field": out, "dx": out.dx, "dy": out.dy, "z": z, "magnification": out.dx / dx,
+            "undersampled": under, "zCritical": z_c}
+
+
+def propagateFraunhofer(field: ComplexField, lam, z, opts=None, *, ctx=None, **kw):
+    """src/propagate.js:310-312 (same transform as propagateFresnelFFT)."""
+    return propagateFresnelFFT(field, lam, z, opts, ctx=ctx, **kw)
+
+
+def propagateFresnelFFTInverse(field: ComplexField, lam, z, opts=None, *, ctx=None, **kw):
+    """Exact inverse of propagateFresnelFFT back onto the DOE grid (src/propagate.js:237-308)."""
+    dx = _opt(opts, kw, "dx", None)
+    dy = _opt(opts, kw, "dy", None)
+    if not dx or not dy:
+        raise ValueError("propagateFresnelFFTInverse: pass the DOE-plane pitch as {dx, dy}")
+    c = ctx or _lib.context()
+    out = ComplexField(field.nx, field.ny, dx, dy)
+    c.check(c.lib.doe_fresnel_inverse(c.h, _lib.dp(field.re), _lib.dp(field.im), field.nx, field.ny, field.dx,
+                                      field.dy, float(lam), float(z), float(dx), float(dy), _lib.dp(out.re),
+                                      _lib.dp(out.im)))
+    return out
+
+
 def propagate(field: ComplexField, lam, z, opts=None, *, ctx=None, **kw):
-    """Generic entry point (src/propagate.js:383-389); method 'asm' only."""
+    """Generic entry point (src/propagate.js:383-389): method 'asm' (default) or 'fresnel'."""
     method = _opt(opts, kw, "method", "asm")
     pad = int(_opt(opts, kw, "pad", 1))
-    if method != "asm":
-        raise NotImplementedError("propagate: only method='asm' is provided by this engine")
     src = field
     if pad > 1:
         from .projector import resample_centred
         src = resample_centred(field, field.nx * pad, field.ny * pad)
+    if method == "fresnel":
+        return propagateFresnelFFT(src, lam, z, opts, ctx=ctx, **kw)["field"]
     bl = _opt(opts, kw, "bandLimit", True)
     return propagateAngularSpectrum(src, lam, z, {"bandLimit": True if bl is None else bl}, ctx=ctx)

@@ -111,6 +111,19 @@ int doe_focal_plane(doe_ctx* ctx, const double* re, const double* im, int nx, in
                     double dx, double dy, double lambda, double f, double* out_re,
                     double* out_im, double* out_d);
 
+/* propagateFresnelFFT -- src/propagate.js:155-230: single-FFT Fresnel transform
+ * of the nx*ny FP64 planes to the magnified grid; out_d receives its pitch
+ * {lambda|z|/(nx dx), lambda|z|/(ny dy)}. z must be non-zero. Inputs and outputs
+ * may alias. The undersampling check (throwOnUndersampled) is host-side. */
+int doe_fresnel(doe_ctx* ctx, const double* re, const double* im, int nx, int ny, double dx,
+                double dy, double lambda, double z, double* out_re, double* out_im, double* out_d);
+
+/* propagateFresnelFFTInverse -- src/propagate.js:237-308: the exact inverse,
+ * from the magnified grid (pitch dux, duy) back to the DOE grid (pitch dx, dy). */
+int doe_fresnel_inverse(doe_ctx* ctx, const double* re, const double* im, int nx, int ny,
+                        double dux, double duy, double lambda, double z, double dx, double dy,
+                        double* out_re, double* out_im);
+
 /* ------------------------------------------------------------ device-resident */
 /* Batched 2-D FFT of nplanes complex64 planes in place (device pointer). */
 int doe_fft2d_dev(doe_ctx* ctx, void* d_planes, int nx, int ny, int nplanes, int inverse);
@@ -190,6 +203,19 @@ typedef struct doe_design_dev_desc {
   double* error;     /* [batch][iterations], may be NULL */
   double* efficiency;
   double* rmse;      /* [batch], WGS, may be NULL */
+  /* Per-design stopping goal (image-plane WGS only; no counterpart in the
+   * reference, whose loop always runs `iterations`). When rmse_goal > 0 the
+   * screen RMSE of src/projector.js:554-595 (target scaled to the in-ROI power,
+   * intensity RMSE over the ROI) is measured on every iteration's forward field,
+   * fused into the iteration's last pass; a design whose screen RMSE reaches the
+   * goal returns that iterate and drops out of all later passes. screen_irr is
+   * the target irradiance [batch][nx*ny] (NULL: target_amp^2, equivalent for the
+   * scale-invariant RMSE). iterations_used [batch] (may be NULL) receives the
+   * iterations each design ran; error/efficiency entries past that repeat the
+   * last value. */
+  double rmse_goal;
+  const float* screen_irr;
+  int* iterations_used;
 } doe_design_dev_desc;
 int doe_design_dev(doe_ctx* ctx, const doe_design_dev_desc* desc);
 
@@ -203,6 +229,30 @@ int doe_multiplane(doe_ctx* ctx, int nx, int ny, double dx, double dy, double la
                    const double* target_amp, const double* roi, const double* weight,
                    int iterations, const double* init_phase, double* phase, double* error,
                    double* efficiency, double* per_plane_error);
+
+/* Batched, device-resident gerchbergSaxtonMultiPlane: B designs of one grid and
+ * one set of planes (z, weight: host arrays of nplanes; weight may be NULL).
+ * Device FP32 planes: illumination [batch][n], target_amp and roi
+ * [batch][nplanes][n] (roi may be NULL), phase [batch][n] (initial phase in,
+ * result out). Device FP64 outputs (may be NULL): error and efficiency
+ * [batch][iterations], per_plane_error [batch][nplanes][iterations].
+ * Asynchronous on the context's stream. */
+typedef struct doe_multiplane_dev_desc {
+  int batch, nx, ny;
+  double dx, dy, lambda;
+  int nplanes;
+  const double* z;
+  const double* weight;
+  int iterations;
+  const float* illumination;
+  const float* target_amp;
+  const float* roi;
+  float* phase;
+  double* error;
+  double* efficiency;
+  double* per_plane_error;
+} doe_multiplane_dev_desc;
+int doe_multiplane_dev(doe_ctx* ctx, const doe_multiplane_dev_desc* desc);
 
 /* ------------------------------------------------------------ projector */
 /* ProjectorSystem.simulate -- src/projector.js:475-498: the element A exp(i phi)

@@ -599,8 +599,48 @@ int orc_fourier_cgh(const double* illumination, const double* targetAmp,
 }
 
 /* src/doe.js:455-546 */
+/* Screen RMSE of src/projector.js:554-595 on an intensity plane (the pitch
+ * cancels): target scaled to the in-ROI power, RMSE over the ROI. */
+static double screen_rmse(const double* inten, const double* T, const double* roi, long n) {
+  double im = 0, tt = 0, ii = 0, it = 0, t2 = 0;
+  for (long k = 0; k < n; k++) {
+    double m = roi ? roi[k] : 1;
+    im += inten[k] * m;
+    tt += T[k];
+    if (m > 0) {
+      ii += inten[k] * inten[k];
+      it += inten[k] * T[k];
+      t2 += T[k] * T[k];
+    }
+  }
+  double s = tt > 0 ? im / tt : 0;
+  double den = s * s * t2;
+  double num = fmax(0.0, ii - 2 * s * it + s * s * t2);
+  return den > 0 ? sqrt(num / den) : 0;
+}
+
+static int weighted_gs_impl(const double* illumination, const double* targetAmp,
+                            const orc_design_opts* o, int base, const double* screen_irr,
+                            double goal, int* used, orc_design_result* r);
+
 int orc_weighted_gs(const double* illumination, const double* targetAmp,
                     const orc_design_opts* o, int base, orc_design_result* r) {
+  return weighted_gs_impl(illumination, targetAmp, o, base, NULL, 0.0, NULL, r);
+}
+
+/* Image-plane WGS with the engine's per-design stopping goal (no counterpart in
+ * the reference): after every iteration the screen RMSE of its forward field is
+ * measured; at or below `goal` that iterate is returned and the loop ends.
+ * screen_irr NULL uses targetAmp^2. *used receives the iterations run. */
+int orc_weighted_gs_goal(const double* illumination, const double* targetAmp,
+                         const orc_design_opts* o, const double* screen_irr, double goal,
+                         int* used, orc_design_result* r) {
+  return weighted_gs_impl(illumination, targetAmp, o, 0, screen_irr, goal, used, r);
+}
+
+static int weighted_gs_impl(const double* illumination, const double* targetAmp,
+                            const orc_design_opts* o, int base, const double* screen_irr,
+                            double goal, int* used, orc_design_result* r) {
   int nx = o->nx, ny = o->ny;
   long n = (long)nx * ny;
   const double* roi = o->roi;
@@ -619,6 +659,14 @@ int orc_weighted_gs(const double* illumination, const double* targetAmp,
   double bestRmse = INFINITY;
   int have_best = 0;
   double beta = o->beta;
+  double* T2 = NULL;
+  if (goal > 0 && !screen_irr) {
+    T2 = (double*)malloc(sizeof(double) * n);
+    if (!T2) return -2;
+    for (long k = 0; k < n; k++) T2[k] = targetAmp[k] * targetAmp[k];
+    screen_irr = T2;
+  }
+  int ran = o->iterations;
   for (int it = 0; it < o->iterations; it++) {
     orc_design_opts so = *o;
     so.weights = weights;
@@ -642,7 +690,8 @@ int orc_weighted_gs(const double* illumination, const double* targetAmp,
       den += targetAmp[k] * targetAmp[k];
     }
     double rmse = den > 0 ? sqrt(num / den) : 0;
-    if (rmse < bestRmse) {
+    int stop = goal > 0 && screen_rmse(inten, screen_irr, roi, n) <= goal;
+    if (rmse < bestRmse || stop) {
       bestRmse = rmse;
       memcpy(best_phase, cur_phase, sizeof(double) * n);
       memcpy(best_amp, amp, sizeof(double) * n);
@@ -665,7 +714,17 @@ int orc_weighted_gs(const double* illumination, const double* targetAmp,
     for (long k = 0; k < n; k++) weights[k] *= nrm;
     if (r->error) r->error[it] = bestRmse;
     if (r->efficiency) r->efficiency[it] = eff[0];
+    if (stop) {
+      ran = it + 1;
+      for (int j = it + 1; j < o->iterations; j++) {
+        if (r->error) r->error[j] = bestRmse;
+        if (r->efficiency) r->efficiency[j] = eff[0];
+      }
+      break;
+    }
   }
+  if (used) *used = ran;
+  free(T2);
   if (have_best) {
     memcpy(r->phase, best_phase, sizeof(double) * n);
     if (r->amplitude) memcpy(r->amplitude, best_amp, sizeof(double) * n);

@@ -105,6 +105,10 @@ int orc_fourier_cgh(const double* illumination, const double* target_amp,
 /* src/doe.js:455-546; base = 0 gerchbergSaxton, 1 fourierCgh */
 int orc_weighted_gs(const double* illumination, const double* target_amp,
                     const orc_design_opts* o, int base, orc_design_result* r);
+/* Image-plane WGS stopped at a screen-RMSE goal (engine extension, see the .c). */
+int orc_weighted_gs_goal(const double* illumination, const double* target_amp,
+                         const orc_design_opts* o, const double* screen_irr, double goal,
+                         int* used, orc_design_result* r);
 /* src/doe.js:557-626. Plane p uses z[p], target_amp + p*n, roi + p*n (roi may be NULL),
  * weight[p]. per_plane_error is nplanes*iterations (row p = plane p). */
 int orc_gs_multiplane(const double* illumination, int nplanes, const double* z,

@@ -81,6 +81,8 @@ def lib():
         L.orc_gerchberg_saxton.argtypes = [_dp, _dp, C.POINTER(DesignOpts), C.POINTER(DesignResult)]
         L.orc_fourier_cgh.argtypes = [_dp, _dp, C.POINTER(DesignOpts), C.POINTER(DesignResult)]
         L.orc_weighted_gs.argtypes = [_dp, _dp, C.POINTER(DesignOpts), i, C.POINTER(DesignResult)]
+        L.orc_weighted_gs_goal.argtypes = [_dp, _dp, C.POINTER(DesignOpts), _dp, d, C.POINTER(i),
+                                           C.POINTER(DesignResult)]
         L.orc_gs_multiplane.argtypes = [_dp, i, _dp, _dp, _dp, _dp, C.POINTER(DesignOpts),
                                         _dp, _dp, _dp, _dp]
         L.orc_auto_roi.argtypes = [_dp, i, i, d, d, d, _dp]
@@ -232,11 +234,13 @@ def _opts(nx, ny, dx, dy, lam, z, iterations, feedback=0.0, escape=0, beta=0.9, 
 
 def design(algorithm, illumination, target_amp, *, nx, ny, dx, dy=None, lam=532e-9, z=0.03,
            iterations=60, feedback=0.0, escape=0, beta=0.9, seed=12345, roi=None,
-           weights=None, init_phase=None):
+           weights=None, init_phase=None, rmse_goal=0.0, screen_irr=None):
     """Run gs / wgs / fourier / wgs-fourier with the reference's semantics.
 
     algorithm: 'gs' (src/doe.js:327), 'fourier' (:639), 'wgs' (:455 over gs),
-    'wgs-fourier' (:455 over fourierCgh).
+    'wgs-fourier' (:455 over fourierCgh). rmse_goal > 0 ('wgs' only) stops at the
+    first iteration whose screen RMSE meets it (the engine's stopping rule) and
+    reports `iterationsUsed`.
     """
     dy = dx if dy is None else dy
     ill, tgt = _f64(illumination), _f64(target_amp)
@@ -257,6 +261,12 @@ def design(algorithm, illumination, target_amp, *, nx, ny, dx, dy=None, lam=532e
         rc = L.orc_gerchberg_saxton(_p(ill), _p(tgt), C.byref(o), C.byref(r))
     elif algorithm == "fourier":
         rc = L.orc_fourier_cgh(_p(ill), _p(tgt), C.byref(o), C.byref(r))
+    elif algorithm == "wgs" and rmse_goal > 0:
+        used = C.c_int(0)
+        sirr = None if screen_irr is None else _f64(screen_irr)
+        rc = L.orc_weighted_gs_goal(_p(ill), _p(tgt), C.byref(o), _p(sirr), float(rmse_goal), C.byref(used),
+                                    C.byref(r))
+        res["iterationsUsed"] = used.value
     elif algorithm in ("wgs", "wgs-fourier"):
         rc = L.orc_weighted_gs(_p(ill), _p(tgt), C.byref(o), int(algorithm == "wgs-fourier"),
                                C.byref(r))

@@ -215,3 +215,100 @@ def test_design_rejects_unsupported_grids(engine):
         engine.gerchbergSaxton(np.ones(16 * 16), np.ones(16 * 16), {"nx": 16, "iterations": 2})
     with pytest.raises(ValueError, match="no planes"):
         engine.gerchbergSaxtonMultiPlane(np.ones(64 * 64), [], {"nx": 64})
+
+
+# ------------------------------------------------------------------ screen-RMSE stopping goal
+def _goal_batch(engine, oracle, B=6, n=64, seed0=11):
+    import torch
+    ill = oracle.disc_mask(n, n, DX, DX, 0.45 * n * DX, 2 * DX)
+    irr = [disc(n, 8 + 2 * k) for k in range(B)]
+    tgt = np.array([oracle.prepare_target(t, ill) for t in irr])
+    roi = np.array([oracle.auto_roi(t, n, n) for t in irr])
+    ph = np.array([oracle.random_phase(n, n, seed0 + k) for k in range(B)])
+    f = lambda a: torch.tensor(np.asarray(a, dtype=np.float32), device="cuda").reshape(B, -1).contiguous()
+    return (torch.tensor(ill.astype(np.float32), device="cuda"), f(tgt), f(roi), f(ph), f(np.array(irr)))
+
+
+def test_wgs_rmse_goal_stops_each_design_at_its_goal(engine, oracle):
+    """Per-design early stop: every stopped design's returned screen meets the goal,
+    its iterate equals the goal-free run of the same length, and designs that run
+    on are unaffected by the others dropping out."""
+    from diffractiveopticalelement_b200 import batch
+    c = engine.context()
+    n, B, I = 64, 6, 40
+    ill, tgt, roi, ph0, irr = _goal_batch(engine, oracle, B, n)
+    kw = dict(nx=n, ny=n, dx=DX, lam=LAMBDA, z=0.03, roi=roi)
+    free = batch.design_batch(c, ill, tgt, ph0.clone(), iterations=I, **kw)
+    m_free = batch.screen_metrics_batch(c, free["amplitude"], irr, ill, nx=n, ny=n, sdx=DX, roi=roi)[:, 0].cpu()
+    goal = float(np.median(m_free.numpy()))  # some designs stop, some run on
+    got = batch.design_batch(c, ill, tgt, ph0.clone(), iterations=I, rmse_goal=goal, screen_irr=irr, **kw)
+    used = got["iterations_used"].cpu().numpy()
+    m_got = batch.screen_metrics_batch(c, got["amplitude"], irr, ill, nx=n, ny=n, sdx=DX, roi=roi)[:, 0].cpu()
+    stopped = used < I
+    assert stopped.any() and (~stopped).any()
+    for k in range(B):
+        if stopped[k]:
+            assert m_got[k] <= goal * (1 + 1e-6)
+            # the same design run for exactly `used` iterations without a goal
+            one = batch.design_batch(c, ill, tgt[k:k + 1].clone(), ph0[k:k + 1].clone(), iterations=int(used[k]),
+                                     nx=n, ny=n, dx=DX, lam=LAMBDA, z=0.03, roi=roi[k:k + 1].clone())
+            assert torch_equal(one["phase"][0], got["phase"][k])
+            err = got["error"][k].cpu().numpy()
+            assert np.all(err[used[k]:] == err[used[k] - 1])
+        else:
+            assert used[k] == I
+            assert torch_equal(free["phase"][k], got["phase"][k])
+            assert torch_equal(free["amplitude"][k], got["amplitude"][k])
+
+
+def test_wgs_rmse_goal_rejected_outside_image_plane_wgs(engine, oracle):
+    from diffractiveopticalelement_b200 import DOEError, batch
+    c = engine.context()
+    ill, tgt, roi, ph0, irr = _goal_batch(engine, oracle, 2, 64)
+    with pytest.raises(DOEError, match="goal"):
+        batch.design_batch(c, ill, tgt, ph0, nx=64, ny=64, dx=DX, iterations=4, algorithm="gs", rmse_goal=0.01)
+
+
+def torch_equal(a, b):
+    import torch
+    return bool(torch.equal(a, b))
+
+
+def test_wgs_rmse_goal_stop_iteration_matches_oracle(engine, oracle):
+    """The stop iteration of the goal rule agrees with the FP64 oracle's (same rule)."""
+    from diffractiveopticalelement_b200 import batch
+    c = engine.context()
+    n, B, I, goal = 64, 4, 60, 0.02
+    ill, tgt, roi, ph0, irr = _goal_batch(engine, oracle, B, n, seed0=31)
+    got = batch.design_batch(c, ill, tgt, ph0.clone(), nx=n, ny=n, dx=DX, lam=LAMBDA, z=0.03, iterations=I, roi=roi,
+                             rmse_goal=goal, screen_irr=irr)
+    used = got["iterations_used"].cpu().numpy()
+    ill_h = ill.cpu().numpy().astype(np.float64)
+    for k in range(B):
+        r = oracle.design("wgs", ill_h, tgt[k].cpu().numpy(), nx=n, ny=n, dx=DX, lam=LAMBDA, z=0.03, iterations=I,
+                          roi=roi[k].cpu().numpy(), init_phase=ph0[k].cpu().numpy(), rmse_goal=goal,
+                          screen_irr=irr[k].cpu().numpy())
+        assert abs(int(used[k]) - r["iterationsUsed"]) <= 1, (k, used[k], r["iterationsUsed"])
+
+
+def test_multiplane_batch_equals_single_designs(engine, oracle):
+    """doe_multiplane_dev over B designs == B calls of the host multi-plane loop."""
+    import torch
+    from diffractiveopticalelement_b200 import batch
+    n, B, zs, I = 64, 3, [0.02, 0.03, 0.04], 6
+    ill = oracle.disc_mask(n, n, DX, DX, 0.45 * n * DX, 2 * DX)
+    tg = np.array([[oracle.prepare_target(disc(n, 6 + 3 * p + 2 * d), ill) for p in range(3)] for d in range(B)])
+    ro = np.array([[oracle.auto_roi(disc(n, 6 + 3 * p + 2 * d), n, n) for p in range(3)] for d in range(B)])
+    ph = np.array([oracle.random_phase(n, n, 50 + d) for d in range(B)])
+    f = lambda a: torch.tensor(np.asarray(a, dtype=np.float32), device="cuda").contiguous()
+    got = batch.multiplane_batch(engine.context(), f(ill), f(tg).reshape(B * 3, -1), f(ph), zs, nx=n, ny=n, dx=DX,
+                                 lam=LAMBDA, iterations=I, roi=f(ro).reshape(B * 3, -1), weights=[1.0, 0.5, 2.0])
+    for d in range(B):
+        one = engine.gerchbergSaxtonMultiPlane(
+            ill, [{"z": zs[p], "targetAmp": tg[d, p].astype(np.float32).astype(np.float64),
+                   "roi": ro[d, p].astype(np.float32).astype(np.float64), "weight": [1.0, 0.5, 2.0][p]}
+                  for p in range(3)],
+            {"nx": n, "dx": DX, "lambda": LAMBDA, "iterations": I,
+             "initPhase": ph[d].astype(np.float32).astype(np.float64)})
+        assert np.array_equal(got["phase"][d].cpu().numpy().astype(np.float64), one["phase"])
+        assert np.allclose(got["error"][d].cpu().numpy(), one["error"], rtol=1e-12, atol=0)

@@ -176,3 +176,49 @@ def test_errors_use_reference_wording(engine):
                                 3, 4, 0))
     with pytest.raises(DOEError, match="not supported"):
         c.check(c.lib.doe_fft2d(c.h, None, None, 16384, 1, 0))
+
+
+# ------------------------------------------------------------------ single-FFT Fresnel
+def gaussian_phase_field(engine, nx, ny, d, seed):
+    rng = np.random.default_rng(seed)
+    i = (np.arange(nx) - nx / 2) * d
+    j = (np.arange(ny) - ny / 2) * d
+    X, Y = np.meshgrid(i, j)
+    w = 0.2 * nx * d
+    amp = np.exp(-(X ** 2 + Y ** 2) / w ** 2)
+    ph = 3.0 * rng.standard_normal() * (X / (nx * d)) + 5.0 * (X ** 2 + Y ** 2) / (nx * d) ** 2
+    f = engine.ComplexField(nx, ny, d, d)
+    f.re = (amp * np.cos(ph)).ravel().copy()
+    f.im = (amp * np.sin(ph)).ravel().copy()
+    return f
+
+
+@pytest.mark.parametrize("nx,ny,z", [(64, 64, 0.05), (256, 256, 0.03), (128, 64, 0.2), (512, 512, -0.04),
+                                     (32, 128, 0.01)])
+def test_fresnel_matches_oracle(engine, oracle, nx, ny, z):
+    d = 8e-6
+    f = gaussian_phase_field(engine, nx, ny, d, nx + ny)
+    r = engine.propagateFresnelFFT(f, LAMBDA, z)
+    orr, oi, dux, duy = oracle.fresnel(f.re, f.im, nx, ny, d, d, LAMBDA, z)
+    assert rel_l2(r["field"].re + 1j * r["field"].im, orr + 1j * oi) < TOL
+    assert r["dx"] == pytest.approx(dux, rel=1e-15) and r["dy"] == pytest.approx(duy, rel=1e-15)
+    assert r["zCritical"] == pytest.approx(nx * d * d / LAMBDA)
+    assert r["undersampled"] == (abs(z) < r["zCritical"])
+    b = engine.propagateFresnelFFTInverse(r["field"], LAMBDA, z, {"dx": d, "dy": d})
+    br, bi = oracle.fresnel_inverse(orr, oi, nx, ny, dux, duy, LAMBDA, z, d, d)
+    assert rel_l2(b.re + 1j * b.im, br + 1j * bi) < TOL
+    # round trip (test/propagate.test.js:137-146)
+    assert rel_l2(b.re + 1j * b.im, f.re + 1j * f.im) < TOL
+
+
+def test_fresnel_argument_errors(engine):
+    f = engine.ComplexField(64, 64, 8e-6, 8e-6)
+    with pytest.raises(ValueError, match="under-sampled"):
+        engine.propagateFresnelFFT(f, LAMBDA, 1e-4, {"throwOnUndersampled": True})
+    with pytest.raises(ValueError, match="DOE-plane pitch"):
+        engine.propagateFresnelFFTInverse(f, LAMBDA, 0.05, {})
+    from diffractiveopticalelement_b200 import DOEError
+    with pytest.raises(DOEError, match="non-zero"):
+        engine.propagateFresnelFFT(f, LAMBDA, 0.0)
+    g = engine.propagate(gaussian_phase_field(engine, 64, 64, 8e-6, 1), LAMBDA, 0.05, {"method": "fresnel"})
+    assert g.dx == pytest.approx(LAMBDA * 0.05 / (64 * 8e-6))
