@@ -77,6 +77,14 @@ class MultiplaneDevDesc(C.Structure):
                 ("efficiency", _vp), ("per_plane_error", _vp)]
 
 
+
+class PhaseLossDesc(C.Structure):
+    """doe_phase_loss_desc (device-resident FP32 planes)."""
+    _fields_ = [("batch", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("lambda_", C.c_double), ("z", C.c_double), ("illumination", _vp), ("target_amp", _vp),
+                ("roi", _vp), ("phase", _vp), ("grad", _vp), ("loss", _vp)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -112,6 +120,17 @@ def _declare(L):
         "doe_design_batch": (i, [ctxp, i, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
         "doe_multiplane_dev": (i, [ctxp, C.POINTER(MultiplaneDevDesc)]),
+        "doe_phase_loss_grad": (i, [ctxp, C.POINTER(PhaseLossDesc)]),
+        "doe_phase_supervised_grad": (i, [ctxp, C.c_longlong, _vp, _vp, _vp, _vp]),
+        "doe_surrogate_create": (i, [ctxp, i, i, i, i, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+        "doe_surrogate_destroy": (None, [_vp]),
+        "doe_surrogate_param_count": (C.c_longlong, [_vp]),
+        "doe_surrogate_params": (i, [_vp, C.POINTER(C.c_float), i]),
+        "doe_surrogate_set_params": (i, [_vp, C.POINTER(C.c_float)]),
+        "doe_surrogate_forward": (i, [_vp, i, _vp, _vp, _vp]),
+        "doe_surrogate_backward": (i, [_vp, _vp]),
+        "doe_surrogate_zero_grad": (i, [_vp]),
+        "doe_surrogate_adam": (i, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
         "doe_multiplane": (i, [ctxp, i, i, d, d, d, _dp, i, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]),
         "doe_autotune": (i, [ctxp, i, i, d, d, d, d, C.POINTER(C.c_int)]),
         "doe_ctx_set_tuning": (i, [ctxp, C.c_char_p, C.c_longlong]),
@@ -144,7 +163,7 @@ def declared_functions() -> list[str]:
     """Entry points declared in include/doe_b200.h."""
     import re
     src = open(HEADER).read()
-    return re.findall(r"^\s*(?:int|void|const char\s*\*|void\s*\*)\s*(doe_\w+)\s*\(", src, re.M)
+    return re.findall(r"^\s*(?:int|void|long long|const char\s*\*|void\s*\*)\s*(doe_\w+)\s*\(", src, re.M)
 
 
 class Context:

@@ -155,6 +155,32 @@ static int carve_state(doe_ctx* c, DesignBufs& b, int B, int Ih, int bpp, int pp
   return DOE_OK;
 }
 
+// Work plane, one transfer table and reduction state for B designs of one
+// geometry (the phase-gradient passes); planes are attached by the caller.
+int design_prepare(doe_ctx* c, DesignBufs& b, int B, int nx, int ny, double dx, double dy, const double* lam,
+                   const double* z, int ntab, bool wgs, bool needU) {
+  (void)wgs;
+  (void)needU;
+  DOE_TRY(check_design_grid(c, nx, ny, "phase loss"));
+  const long n = (long)nx * ny;
+  void* p0;
+  DOE_TRY(ensure_slot(c, kSlotDesign0, (size_t)B * n * sizeof(float2) + (size_t)ntab * n * sizeof(float2) + 1024, &p0));
+  char* q0 = (char*)p0;
+  memset(&b, 0, sizeof(b));
+  b.nx = nx;
+  b.ny = ny;
+  b.iters = 1;
+  b.dx = dx;
+  b.dy = dy;
+  b.tgt_stride = n;
+  b.W = (float2*)take(q0, (size_t)B * n * sizeof(float2));
+  float2* htab = (float2*)take(q0, (size_t)ntab * n * sizeof(float2));
+  b.htab = htab;
+  b.htab_stride = ntab > 1 ? n : 0;
+  DOE_TRY(carve_state(c, b, B, 1, design_bpp(nx, ny), 0));
+  return build_htab(c, nx, ny, dx, dy, ntab, lam, z, htab);
+}
+
 }  // namespace doe
 
 using namespace doe;

@@ -536,6 +536,83 @@ struct RowWgsConstrain : NoReduce {
   __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.W[x] = v; }
 };
 
+// ------------------------------------------------------------------ phase gradient
+// Intensity loss of a DOE phase and its gradient (no reference counterpart; the
+// training signal of the warm-start surrogate). With U0 = A exp(i phi), U = P U0
+// (P the image-plane propagation of the design loops) and I = |U|^2:
+//   L = sum m (I - T)^2 / sum m T^2,   T = t^2,
+//   dL/dU* = 2 m (I - T) U / D,  dL/dphi = 2 Im(conj(U0) P^H(dL/dU*)),  D = sum m T^2.
+// Pass 3 of 5: inverse row FFT gives U; FP64 sums of the numerator and D; the
+// unnormalised G = 2 m (I - T) U goes through the forward row FFT of P^H.
+struct RowLossField {
+  static constexpr const char* kName = "design_row_loss";
+  static constexpr int kStages = 2;
+  static constexpr bool kInv1 = true, kInv2 = false;
+  using Acc = DesignAcc;
+  DesignBufs b;
+  float scale;
+  struct State {
+    const float* t;
+    const float* m;
+    float2* w;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * b.pe() + (long)y * b.nx;
+    const long ot = p * b.tgt_stride + (long)y * b.nx;
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.W + o};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
+  __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc& acc) const {
+    const float m = s.m ? __ldg(&s.m[x]) : 1.f;
+    const float t = __ldg(&s.t[x]);
+    const float2 u = cscale(v, scale);
+    const float I = u.x * u.x + u.y * u.y, T = t * t;
+    const float r = I - T;
+    acc.v[kErrNum] += (double)m * r * r;
+    acc.v[kErrDen] += (double)m * T * T;
+    v = cscale(u, 2.f * m * r);
+  }
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const { s.w[x] = v; }
+  __device__ __forceinline__ void finish(int p, int bip, int bpp, Acc& acc) const {
+    design_reduce(b, p, bip, bpp, acc);
+  }
+};
+
+// Pass 5 of 5: inverse row FFT gives g0 = P^H G; dphi = 2 Im(conj(U0) g0) / D.
+struct RowPhaseGrad : NoReduce {
+  static constexpr const char* kName = "design_row_phase_grad";
+  static constexpr int kStages = 1;
+  static constexpr bool kInv1 = true, kInv2 = false;
+  DesignBufs b;
+  float scale;
+  float* grad;   // [B][n]
+  double* loss;  // [B] or null
+  struct State {
+    const float* A;
+    const float* ph;
+    float* g;
+    float2* w;
+    float inv_d;
+  };
+  __device__ __forceinline__ State init(int p, int y) const {
+    const long o = p * b.pe() + (long)y * b.nx;
+    const double* T = b.totals + (long)p * kRedK;  // written by RowLossField's reduction
+    const float inv = T[kErrDen] > 0 ? (float)(1.0 / T[kErrDen]) : 0.f;
+    if (loss && y == 0 && threadIdx.x == 0) loss[p] = T[kErrDen] > 0 ? T[kErrNum] / T[kErrDen] : 0.0;
+    return {b.illum + o, b.phase + o, grad + o, b.W + o, inv};
+  }
+  __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
+  __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
+  __device__ __forceinline__ void store(const State& s, int x, float2 v, Acc&) const {
+    const float2 g0 = cscale(v, scale);
+    float sn, cs;
+    sincosf(__ldg(&s.ph[x]), &sn, &cs);
+    const float a = __ldg(&s.A[x]);
+    // Im(conj(a e^{i phi}) g0) = a (cos phi g0.y - sin phi g0.x)
+    s.g[x] = 2.f * a * (cs * g0.y - sn * g0.x) * s.inv_d;
+  }
+};
+
 // Design loops are compiled for power-of-two axes 32..4096 with the default CTA
 // shapes (each operator is instantiated once per size).
 constexpr int kDesignMinN = 32, kDesignMaxN = 4096;

@@ -280,6 +280,52 @@ int doe_screen_metrics_dev(doe_ctx* ctx, int batch, int nx, int ny, const float*
                            const float* illumination, long long illumination_stride, double sdx,
                            double sdy, double dx, double dy, double* out);
 
+/* ------------------------------------------------------------ warm-start surrogate */
+/* No counterpart in the reference. Intensity loss of B DOE phases through the
+ * image-plane propagation of the design loops (bandLimit false) and its gradient:
+ *   L = sum m (|U|^2 - t^2)^2 / sum m t^4,  U = P(A e^{i phase}),
+ * grad = dL/dphase. Device FP32 planes [batch][nx*ny] (roi may be NULL); loss is a
+ * device FP64 array [batch] (may be NULL). Asynchronous on the context's stream. */
+typedef struct doe_phase_loss_desc {
+  int batch, nx, ny;
+  double dx, dy, lambda, z;
+  const float* illumination;
+  const float* target_amp;
+  const float* roi;
+  const float* phase;
+  float* grad;
+  double* loss;
+} doe_phase_loss_desc;
+int doe_phase_loss_grad(doe_ctx* ctx, const doe_phase_loss_desc* desc);
+
+/* A U-Net (levels of base << l channels, 3x3 convolutions + ReLU, 2x2 average
+ * pooling, nearest up-sampling, skip concatenation, 1x1 head to (c, s), phase =
+ * atan2(s, c)) with BF16 weights and activations, FP32 accumulation and FP32
+ * master weights under Adam. Input: target irradiance (scaled by its maximum) and
+ * ROI planes of n x n (plus a constant plane). All device arrays; calls are asynchronous on the context's
+ * stream except the parameter copies. */
+typedef struct doe_surrogate doe_surrogate;
+int doe_surrogate_create(doe_ctx* ctx, int n, int base, int levels, int max_batch,
+                         unsigned long long seed, doe_surrogate** out);
+void doe_surrogate_destroy(doe_surrogate* s);
+long long doe_surrogate_param_count(const doe_surrogate* s);
+/* which = 0: FP32 weights, 1: accumulated gradients (host array of param_count) */
+int doe_surrogate_params(doe_surrogate* s, float* host_out, int which);
+int doe_surrogate_set_params(doe_surrogate* s, const float* host_in);
+int doe_surrogate_forward(doe_surrogate* s, int batch, const float* d_irr, const float* d_roi,
+                          float* d_phase);
+/* back-propagates d_dphase = dL/dphase [batch][n*n] of the last forward pass and
+ * accumulates the parameter gradients */
+int doe_surrogate_backward(doe_surrogate* s, const float* d_dphase);
+int doe_surrogate_zero_grad(doe_surrogate* s);
+/* Adam with decoupled weight decay on grad * grad_scale; zeroes the gradients */
+int doe_surrogate_adam(doe_surrogate* s, float lr, float beta1, float beta2, float eps,
+                       float weight_decay, float grad_scale);
+/* supervised phase loss L = mean(1 - cos(phase - target)) over B*n pixels:
+ * grad = sin(phase - target) / (B n); loss (device FP64 [1], may be NULL) */
+int doe_phase_supervised_grad(doe_ctx* ctx, long long count, const float* d_phase,
+                              const float* d_target, float* d_grad, double* d_loss);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. Angular-spectrum propagation of one complex64
  * plane for callers that must not allocate device memory (a host runtime that owns

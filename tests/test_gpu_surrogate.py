@@ -1,0 +1,133 @@
+"""GPU kernels of the warm-start surrogate against the CPU oracles.
+
+* the network's forward phase and every parameter gradient against the NumPy
+  oracle (oracle/unet_oracle.py) run on the same weights with the GPU's BF16
+  rounding points (tolerances below: BF16 activations, FP32 accumulation);
+* the physics loss and its phase gradient against an FP64 restatement through
+  the oracle's angular-spectrum propagation (1e-5 / 1e-4);
+* one Adam step against the update formula.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import unet_oracle as U
+
+pytestmark = pytest.mark.gpu
+DX, LAM, Z = 8e-6, 532e-9, 0.03
+
+
+def _inputs(n, B, seed):
+    rng = np.random.default_rng(seed)
+    irr = (rng.random((B, n * n)) ** 3).astype(np.float32)
+    roi = (rng.random((B, n * n)) > 0.4).astype(np.float32)
+    return irr, roi
+
+
+@pytest.mark.parametrize("n,base,levels,B", [(32, 32, 3, 2), (64, 32, 4, 3), (16, 64, 2, 1)])
+def test_forward_and_gradients_match_oracle(engine, n, base, levels, B):
+    import torch
+    from diffractiveopticalelement_b200.surrogate import Surrogate
+    s = Surrogate(n=n, base=base, levels=levels, max_batch=B, seed=11)
+    p = s.params()
+    assert p.size == U.param_count(base, levels)
+    irr, roi = _inputs(n, B, n + levels)
+    d_irr, d_roi = torch.tensor(irr, device="cuda"), torch.tensor(roi, device="cuda")
+    ph = s.forward(d_irr, d_roi).cpu().numpy()
+    net = U.UNet(p, n, base, levels, emu=True)
+    ph_o = net.forward(irr, roi)
+    assert rel_l2(np.exp(1j * ph), np.exp(1j * ph_o)) < 2e-2
+    assert np.median(np.abs(np.angle(np.exp(1j * (ph - ph_o))))) < 1e-2
+    rng = np.random.default_rng(3)
+    dphase = rng.standard_normal((B, n * n)).astype(np.float32)
+    # d atan2(s, c) scales with 1 / (c^2 + s^2): drop the pixels where (c, s) is
+    # near the origin, whose gradients amplify the FP32-vs-FP64 forward differences
+    r2 = (net.S["c"] ** 2 + net.S["s"] ** 2).reshape(B, -1)
+    dphase[r2 < 0.25 * np.median(r2)] = 0.0
+    s.zero_grad()
+    s.backward(torch.tensor(dphase, device="cuda"))
+    g = s.gradients().astype(np.float64)
+    g_o = net.backward(dphase)
+    # BF16 activations: a value whose FP32 sum lands on the other side of a BF16
+    # rounding boundary than the oracle's FP64 sum differs by one BF16 ulp, and the
+    # deep chain spreads that; the bounds below sit well inside what a wrong
+    # transpose, flip, mask or scale produces (cosine near 0 or a ratio far from 1)
+    cos = lambda x, y: float(x @ y / (np.linalg.norm(x) * np.linalg.norm(y) + 1e-300))
+    print("overall rel", rel_l2(g, g_o), "cos", cos(g, g_o))
+    assert rel_l2(g, g_o) < 0.2 and cos(g, g_o) > 0.99
+    o = 0
+    for ci, co in U.layer_shapes(base, levels):  # per layer, so no layer hides behind the others
+        k = co * 9 * ci
+        print((ci, co), rel_l2(g[o:o + k], g_o[o:o + k]), cos(g[o:o + k], g_o[o:o + k]))
+        assert rel_l2(g[o:o + k], g_o[o:o + k]) < 0.3 and cos(g[o:o + k], g_o[o:o + k]) > 0.97, (ci, co)
+        assert rel_l2(g[o + k:o + k + co], g_o[o + k:o + k + co]) < 0.3, (ci, co, "bias")
+        o += k + co
+    assert rel_l2(g[o:], g_o[o:]) < 2e-2  # head
+    s.close()
+
+
+def test_adam_step_matches_formula(engine):
+    import torch
+    from diffractiveopticalelement_b200.surrogate import Surrogate
+    s = Surrogate(n=16, base=32, levels=2, max_batch=1, seed=2)
+    irr, roi = _inputs(16, 1, 9)
+    p0 = s.params().astype(np.float64)
+    s.forward(torch.tensor(irr, device="cuda"), torch.tensor(roi, device="cuda"))
+    s.zero_grad()
+    s.backward(torch.ones((1, 256), device="cuda"))
+    g = s.gradients().astype(np.float64)
+    lr, b1, b2, eps, wd, gs = 1e-3, 0.9, 0.999, 1e-8, 1e-4, 0.5
+    s.adam(lr, b1, b2, eps, wd, gs)
+    p1 = s.params().astype(np.float64)
+    gg = g * gs
+    m, v = (1 - b1) * gg, (1 - b2) * gg * gg
+    want = p0 - lr * ((m / (1 - b1)) / (np.sqrt(v / (1 - b2)) + eps) + wd * p0)
+    assert np.max(np.abs(p1 - want)) < 1e-6
+    assert np.all(s.gradients() == 0)
+    s.close()
+
+
+def _asm(oracle, f, n, z):
+    r, i = oracle.asm(f.real.copy(), f.imag.copy(), n, n, DX, DX, LAM, z, band_limit=False)
+    return r + 1j * i
+
+
+def phase_loss_fp64(oracle, phase, ill, tgt, roi, n):
+    u0 = ill * np.exp(1j * phase)
+    u = _asm(oracle, u0, n, Z)
+    I, T = np.abs(u) ** 2, tgt ** 2
+    D = np.sum(roi * T * T)
+    L = np.sum(roi * (I - T) ** 2) / D
+    G = 2 * roi * (I - T) * u
+    g0 = _asm(oracle, G, n, -Z)  # P^H: conjugate transfer function
+    return L, 2 * np.imag(np.conj(u0) * g0) / D
+
+
+def test_phase_loss_gradient_matches_fp64(engine, oracle):
+    import torch
+    from diffractiveopticalelement_b200.surrogate import phase_loss_grad
+    n, B = 64, 3
+    rng = np.random.default_rng(1)
+    ill = oracle.disc_mask(n, n, DX, DX, 0.45 * n * DX, 2 * DX)
+    tg = [oracle.prepare_target((rng.random(n * n) > 0.7).astype(float), ill) for _ in range(B)]
+    ro = [(rng.random(n * n) > 0.2).astype(float) for _ in range(B)]
+    ph = [rng.uniform(-np.pi, np.pi, n * n) for _ in range(B)]
+    f32 = lambda a: torch.tensor(np.asarray(a, dtype=np.float32), device="cuda")
+    loss, grad = phase_loss_grad(engine.context(), f32(ph), f32(ill), f32(tg), f32(ro), nx=n, ny=n, dx=DX, lam=LAM, z=Z)
+    loss, grad = loss.cpu().numpy(), grad.cpu().numpy()
+    for k in range(B):
+        q = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+        L, g = phase_loss_fp64(oracle, q(ph[k]), q(ill), q(tg[k]), q(ro[k]), n)
+        assert abs(loss[k] - L) / L < 1e-5
+        assert rel_l2(grad[k], g) < 1e-4
+
+
+def test_supervised_gradient(engine):
+    import torch
+    from diffractiveopticalelement_b200.surrogate import supervised_grad
+    rng = np.random.default_rng(4)
+    a, b = rng.uniform(-3, 3, 5000).astype(np.float32), rng.uniform(-3, 3, 5000).astype(np.float32)
+    loss, g = supervised_grad(engine.context(), torch.tensor(a, device="cuda"), torch.tensor(b, device="cuda"))
+    d = a.astype(np.float64) - b
+    assert abs(loss.item() - np.mean(1 - np.cos(d))) < 1e-6
+    assert np.max(np.abs(g.cpu().numpy() - np.sin(d) / d.size)) < 1e-9
