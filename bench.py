@@ -185,6 +185,7 @@ def main_wgs(args, ctx, device, rank, world, local):
         reached = int(t.item())
     value = reached / (ms / 1e3)
     r.pop("_used")
+    warm = run_warm(ctx, device, args.designs, args.surrogate_steps) if args.surrogate_steps > 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = wgs_cpu_baseline()
@@ -198,7 +199,8 @@ def main_wgs(args, ctx, device, rank, world, local):
                            "pitch_um": 8, "lambda_nm": 532, "z_mm": 30,
                            "targets": "3-8 seeded rectangles 4-40 px in the central 128^2", "band_limit": False,
                            "l2_flush": f"{args.designs} designs x 4 MiB of state exceed L2"},
-                "clocks": clocks, "wgs256": r, "fixed_100_iterations": fixed, "cpu_baseline": cpu, "e2e": None,
+                "clocks": clocks, "wgs256": r, "fixed_100_iterations": fixed, "surrogate_warm_start": warm,
+                "cpu_baseline": cpu, "e2e": None,
                 "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -332,6 +334,156 @@ def main_multiplane(args, ctx, device, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------- uneven far-field batch
+UN_COUNT, UN_ITERS, UN_DX, UN_LAM = 512, 200, 8e-6, 532e-9
+UN_SIZES, UN_PROBS = (128, 256, 512, 1024), (0.4, 0.3, 0.2, 0.1)
+UN_METRIC = "far-field GS designs/s, 512 designs of uneven size (128^2-1024^2), one graph launch"
+UN_CONFIG = {"workload": "farfield_uneven", "designs": UN_COUNT, "sizes": list(UN_SIZES), "probabilities": list(UN_PROBS),
+             "iterations": UN_ITERS, "algorithm": "fourierCgh (designDOE far-field default)", "pitch_um": 8,
+             "lambda_nm": 532, "z": "N dx^2 / lambda (src/projector.js:359-361)",
+             "targets": "seeded k x k Gaussian spot arrays (sigma 1.5 px, k 4..32, weights 1 or U[0.5, 1]) in the "
+                        "central half window, ROI autoRoi", "illumination": "designDOE default disc",
+             "l2_flush": "512 designs of state (~3 GB) exceed L2"}
+
+
+def uneven_specs(seed=7):
+    from diffractiveopticalelement_b200.doe import makeRng
+    rng = makeRng(seed)
+    cum = np.cumsum(UN_PROBS)
+    sizes = []
+    for _ in range(UN_COUNT):
+        u = rng()
+        sizes.append(UN_SIZES[int(np.searchsorted(cum, u, side="right"))] if u < cum[-1] else UN_SIZES[-1])
+    return sizes
+
+
+def uneven_inputs(sizes):
+    """Per size class: illumination, target amplitudes, ROIs, initial phases, irradiance."""
+    import diffractiveopticalelement_b200 as E
+    from diffractiveopticalelement_b200 import surrogate as S
+    from diffractiveopticalelement_b200.projector import autoRoi
+    out = {}
+    for n in UN_SIZES:
+        idx = [k for k, s in enumerate(sizes) if s == n]
+        if not idx:
+            continue
+        ill = E.discMask(n, n, UN_DX, UN_DX, (n * UN_DX / 2) * 0.95, soft=2 * UN_DX)
+        irr = np.array([S.spot_array_target(n, 5000 + k) for k in idx])
+        roi = np.array([autoRoi(t, n, n) for t in irr])
+        tgt = np.array([E.prepareTargetAmp(t, ill) for t in irr])
+        ph = np.array([E.randomPhase(n, n, 5000 + k) for k in idx])
+        out[n] = (ill, irr, roi, tgt, ph)
+    return out
+
+
+def uneven_cpu_baseline(iters=2):
+    """Oracle fourierCgh: one design per size for `iters` iterations on one thread,
+    extrapolated to the workload (counts x 200 iterations) over all host threads."""
+    from oracle import oracle as O
+    O.build()
+    sizes = uneven_specs()
+    inp = uneven_inputs([n for n in UN_SIZES])  # one design per size
+    per_iter = {}
+    for n in UN_SIZES:
+        ill, irr, roi, tgt, ph = inp[n]
+        t0 = time.perf_counter()
+        O.design("fourier", ill, tgt[0], nx=n, ny=n, dx=UN_DX, lam=UN_LAM, z=n * UN_DX ** 2 / UN_LAM,
+                 iterations=iters, roi=roi[0], init_phase=ph[0])
+        per_iter[n] = (time.perf_counter() - t0) / iters
+    threads = os.cpu_count() or 1
+    t1 = sum(per_iter[n] * UN_ITERS for n in sizes)
+    return {"value": UN_COUNT / (t1 / threads), "unit": "designs/s", "cores": threads, "kind": "port",
+            "sample": f"one design per size x {iters} iterations of the FP64 C restatement of fourierCgh on one "
+                      f"thread ({', '.join(f'{n}^2: {1e3 * per_iter[n]:.1f} ms/it' for n in UN_SIZES)}), "
+                      f"extrapolated to the 512-design, 200-iteration workload over {threads} threads"}
+
+
+def main_uneven(args, ctx, device, rank, world, local):
+    """--workload farfield_uneven: 512 far-field GS designs of four sizes in one CUDA-graph launch."""
+    import torch
+    import torch.distributed as dist
+    from diffractiveopticalelement_b200 import batch
+    sizes = uneven_specs(seed=7 + rank)
+    inp = uneven_inputs(sizes)
+    f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
+    classes, ph0 = [], []
+    for n, (ill, irr, roi, tgt, ph) in inp.items():
+        p0 = f32(ph)
+        ph0.append(p0)
+        classes.append({"nx": n, "dx": UN_DX, "lam": UN_LAM, "z": n * UN_DX ** 2 / UN_LAM, "algorithm": "fourier",
+                        "iterations": UN_ITERS, "illumination": f32(ill), "target_amp": f32(tgt), "roi": f32(roi),
+                        "phase": p0.clone()})
+    m = batch.DesignMulti(ctx)
+
+    def reset():
+        for cl, p in zip(classes, ph0):
+            cl["phase"].copy_(p)
+
+    reset()
+    m.run(classes, 0)  # sizes the scratch of every class
+    torch.cuda.synchronize()
+    # direct submission (no graph), for comparison
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reset()
+    e0.record()
+    m.run(classes, 0)
+    e1.record()
+    e1.synchronize()
+    ms_direct = e0.elapsed_time(e1)
+    reset()
+    m.run(classes, 1)  # capture + launch
+    torch.cuda.synchronize()
+    steps = max(1, args.steps if args.steps != 20 else 3)
+    for _ in range(max(args.warmup, 3) - 1):
+        reset()
+        m.run(None, 2)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    n0 = ctx.lib.doe_ctx_launch_count(ctx.h)
+    e0.record()
+    for _ in range(steps):
+        reset()
+        outs = m.run(None, 2)
+    e1.record()
+    e1.synchronize()
+    launches = int(ctx.lib.doe_ctx_launch_count(ctx.h) - n0)
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = UN_COUNT * world / (ms / 1e3)
+    counts = {n: sum(1 for s in sizes if s == n) for n in UN_SIZES}
+    flops = sum(c * 10.0 * n * n * np.log2(n * n) * UN_ITERS for n, c in counts.items())
+    bytes_ = sum(c * 32.0 * n * n * UN_ITERS for n, c in counts.items())
+    peak, peak_kind = peaks()
+    err = np.concatenate([o["error"][:, -1].cpu().numpy() for o in outs])
+    cpu = uneven_cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    if rank == 0:
+        line = {"metric": UN_METRIC, "value": value, "unit": "designs/s", "n_gpus": world, "steps": steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp32 fields, fp64 reductions", "data": "synthetic",
+                "config": dict(UN_CONFIG, counts={str(k): v for k, v in counts.items()}), "clocks": clocks,
+                "roofline": {"bound": "hbm", "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": bytes_ / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                             "basis": "32 B/px per iteration (two FFT passes x 16 B/px), all designs",
+                             "fft_tflops": flops / (ms / 1e3) / 1e12,
+                             "fft_basis": "10 N^2 log2(N^2) FLOP per iteration"},
+                "graph": {"ms_per_step_graph": ms, "ms_per_step_direct": ms_direct,
+                          "kernels_per_step": launches / steps},
+                "final_error": {"median": float(np.median(err)), "max": float(err.max())},
+                "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    m.close()
+    ctx.close()
+    return 0
+
+
 def profile_read(E, ctx):
     names = C.create_string_buffer(64 * 64)
     ms = (C.c_double * 64)()
@@ -387,6 +539,15 @@ def cpu_sample(params, fields_np, nplanes, threads):
 
 def run_reference(args, rank, world):
     if rank != 0:
+        return 0
+    if args.workload == "farfield_uneven":
+        cb = uneven_cpu_baseline()
+        line = {"metric": UN_METRIC, "value": cb["value"], "unit": "designs/s", "n_gpus": args.gpus, "steps": 1,
+                "warmup": 0, "ms_per_step": 1000.0 * UN_COUNT / cb["value"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": UN_CONFIG, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "designs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return 0
     if args.workload == "multiplane2048":
         cb = mp_cpu_baseline()
@@ -557,6 +718,63 @@ def run_wgs(ctx, device, n_designs, warmup, steps, goal=0.0, iters=WGS_ITERS):
 WGS_METRIC = "256^2 image-plane WGS designs/s to screen RMSE<=1% (plain GPU start, batched)"
 
 
+def run_warm(ctx, device, n_designs, steps, goal=0.01):
+    """The surrogate arm: train the U-Net on the GPU (physics loss on a seeded
+    mixture of rectangles / spot arrays / smooth gradients, held apart from the
+    evaluation seeds), then time surrogate inference + WGS to the goal on the same
+    designs as the plain arm. Training time is reported, not timed in the rate."""
+    import torch
+    import diffractiveopticalelement_b200 as E
+    from diffractiveopticalelement_b200 import batch, surrogate as S
+    from diffractiveopticalelement_b200.projector import autoRoi
+    n = WGS_N
+    t0 = time.perf_counter()
+    ill = E.illuminationProfile("rect", n, n, WGS_DX, WGS_DX, {})
+    irr_t = S.training_targets(n, 4096, 1_000_000)
+    roi_t = np.array([autoRoi(t, n, n) for t in irr_t])
+    tgt_t = np.array([E.prepareTargetAmp(t, ill) for t in irr_t])
+    f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
+    d_ill = f32(ill)
+    model = S.Surrogate(n=n, base=32, levels=4, max_batch=16, seed=1, ctx=ctx)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    hist = S.train(model, f32(irr_t), f32(roi_t), d_ill, f32(tgt_t), dx=WGS_DX, lam=WGS_LAM, z=WGS_Z, steps=steps,
+                   batch=16, lr=1e-3, lr_final=1e-4, log_every=max(1, steps // 4))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    _, irr, roi, tgt, ph = wgs_inputs(n_designs)
+    d_irr, d_roi, d_tgt = f32(irr), f32(roi), f32(tgt)
+
+    def step():
+        ph0 = model.forward(d_irr, d_roi)
+        d = batch.design_batch(ctx, d_ill, d_tgt, ph0, nx=n, ny=n, dx=WGS_DX, lam=WGS_LAM, z=WGS_Z,
+                               iterations=WGS_ITERS, roi=d_roi, rmse_goal=goal)
+        m = batch.screen_metrics_batch(ctx, d["amplitude"], d_irr, d_ill, nx=n, ny=n, sdx=WGS_DX, roi=d_roi)
+        return d, m
+
+    step()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    ph0 = model.forward(d_irr, d_roi)
+    e1.record()
+    d = batch.design_batch(ctx, d_ill, d_tgt, ph0, nx=n, ny=n, dx=WGS_DX, lam=WGS_LAM, z=WGS_Z,
+                           iterations=WGS_ITERS, roi=d_roi, rmse_goal=goal)
+    m = batch.screen_metrics_batch(ctx, d["amplitude"], d_irr, d_ill, nx=n, ny=n, sdx=WGS_DX, roi=d_roi)
+    e2.record()
+    e2.synchronize()
+    t_inf, t_all = e0.elapsed_time(e1), e0.elapsed_time(e2)
+    rm = m[:, 0].cpu().numpy()
+    used = d["iterations_used"].cpu().numpy()
+    reached = int(np.sum(rm <= goal))
+    model.close()
+    return {"designs_per_s": reached / (t_all / 1e3), "reached": reached, "ms_per_step": t_all,
+            "inference_ms": t_inf, "iterations_used": {"median": float(np.median(used)), "max": int(used.max())},
+            "network": "U-Net 4 levels 32-256 ch, 2.15M params, BF16 (own kernels), 18.2 GFLOP per 256^2 design",
+            "training": {"steps": steps, "batch": 16, "seconds": t_train, "setup_seconds": t1 - t0,
+                         "loss": "intensity loss through the design propagation (doe_phase_loss_grad)",
+                         "loss_history": hist}}
+
+
 # ----------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -567,9 +785,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-fields", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "wgs256", "multiplane2048"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "wgs256", "multiplane2048", "farfield_uneven"])
     ap.add_argument("--designs", type=int, default=1024, help="designs per step of the WGS workload")
     ap.add_argument("--no-wgs", action="store_true", help="skip the WGS block of the default line")
+    ap.add_argument("--surrogate-steps", type=int, default=1500,
+                    help="training steps of the warm-start surrogate in the wgs256 workload (0: skip the warm arm)")
     ap.add_argument("--fields", type=int, default=NFIELDS,
                     help="fields per step (profiling runs use fewer; the benchmark uses 64)")
     args = ap.parse_args()
@@ -599,6 +819,8 @@ def main():
         return main_wgs(args, ctx, device, rank, world, local)
     if args.workload == "multiplane2048":
         return main_multiplane(args, ctx, device, rank, world, local)
+    if args.workload == "farfield_uneven":
+        return main_uneven(args, ctx, device, rank, world, local)
 
     params = workload_params(seed=2024 + rank)[:max(1, min(args.fields, NFIELDS))]
     nfields = len(params)

@@ -121,6 +121,9 @@ def _declare(L):
         "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
         "doe_multiplane_dev": (i, [ctxp, C.POINTER(MultiplaneDevDesc)]),
         "doe_phase_loss_grad": (i, [ctxp, C.POINTER(PhaseLossDesc)]),
+        "doe_design_multi_create": (i, [ctxp, C.POINTER(C.c_void_p)]),
+        "doe_design_multi_destroy": (None, [_vp]),
+        "doe_design_multi_run": (i, [_vp, i, C.POINTER(DesignDevDesc), i]),
         "doe_phase_supervised_grad": (i, [ctxp, C.c_longlong, _vp, _vp, _vp, _vp]),
         "doe_surrogate_create": (i, [ctxp, i, i, i, i, C.c_ulonglong, C.POINTER(C.c_void_p)]),
         "doe_surrogate_destroy": (None, [_vp]),

@@ -167,3 +167,70 @@ def multiplane_batch(ctx, illumination, target_amp, phase, zs, *, nx, ny, dx, dy
     with _Ordered(ctx):
         ctx.check(ctx.lib.doe_multiplane_dev(ctx.h, C.byref(desc)))
     return {"phase": ph, "error": err, "efficiency": eff, "perPlaneError": ppe}
+
+
+class DesignMulti:
+    """Size classes of designs submitted together (doe_design_multi_*).
+
+    ``run(classes, mode)``: classes is a list of dicts with the keyword arguments of
+    `design_batch` (tensors stay alive in this object until the next run); mode 0
+    runs directly, 1 captures a CUDA graph and launches it, 2 relaunches it.
+    Returns one result dict per class, as `design_batch`.
+    """
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(ctx.lib.doe_design_multi_create(ctx.h, C.byref(h)))
+        self.h = h
+        self._keep = None
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.doe_design_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, classes=None, mode=0):
+        torch = _torch()
+        if mode == 2:
+            with _Ordered(self.ctx):
+                self.ctx.check(self.ctx.lib.doe_design_multi_run(self.h, 0, None, 2))
+            return self._keep[1]
+        descs = (_lib.DesignDevDesc * len(classes))()
+        outs, keep = [], []
+        for k, cl in enumerate(classes):
+            nx, ny = cl["nx"], cl.get("ny", cl["nx"])
+            n = nx * ny
+            ph = cl["phase"]
+            B = ph.shape[0]
+            alg = cl.get("algorithm", "wgs")
+            it = int(cl.get("iterations", 100))
+            ill = _plane(cl["illumination"], B, n, "illumination", shared_ok=True)
+            tgt = _plane(cl["target_amp"], B, n, "target_amp")
+            ro = _plane(cl.get("roi"), B, n, "roi")
+            amp = torch.empty((B, n), dtype=torch.float32, device=ph.device)
+            err = torch.empty((B, max(it, 1)), dtype=torch.float64, device=ph.device)
+            eff = torch.empty_like(err)
+            wgs = alg.startswith("wgs")
+            rmse = torch.empty(B, dtype=torch.float64, device=ph.device) if wgs else None
+            ptr = lambda t: None if t is None else t.data_ptr()
+            descs[k] = _lib.DesignDevDesc(B, nx, ny, cl["dx"], cl.get("dy", cl["dx"]), cl.get("lam", 532e-9),
+                                          cl.get("z", 0.03), None, None, _ALG[alg], it, float(cl.get("feedback", 0.0)),
+                                          int(cl.get("escape", 0)), float(cl.get("beta", 0.9)), ptr(ill), ptr(tgt),
+                                          ptr(ro), ptr(ph), ptr(amp), None, ptr(err), ptr(eff), ptr(rmse), 0.0, None,
+                                          None)
+            o = {"phase": ph, "amplitude": amp, "error": err, "efficiency": eff}
+            if wgs:
+                o["rmse"] = rmse
+            outs.append(o)
+            keep += [ill, tgt, ro, ph, amp, err, eff, rmse]
+        with _Ordered(self.ctx):
+            self.ctx.check(self.ctx.lib.doe_design_multi_run(self.h, len(classes), descs, int(mode)))
+        self._keep = (keep, outs, descs)
+        return outs

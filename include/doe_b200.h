@@ -219,6 +219,19 @@ typedef struct doe_design_dev_desc {
 } doe_design_dev_desc;
 int doe_design_dev(doe_ctx* ctx, const doe_design_dev_desc* desc);
 
+/* Designs of uneven sizes in one submission (no reference counterpart): each
+ * descriptor is one size class (B designs of one grid) and runs on its own
+ * sub-context and stream, forked from and joined into the context's stream.
+ * mode 0 runs directly; mode 1 captures the whole submission (every pass of
+ * every iteration of every class) into a CUDA graph and launches it -- call mode
+ * 0 with the same shapes first so that no scratch is allocated in the capture;
+ * mode 2 relaunches the last captured graph (same descriptors and arrays). */
+typedef struct doe_design_multi doe_design_multi;
+int doe_design_multi_create(doe_ctx* ctx, doe_design_multi** out);
+void doe_design_multi_destroy(doe_design_multi* m);
+int doe_design_multi_run(doe_design_multi* m, int nclasses, const doe_design_dev_desc* descs,
+                         int mode);
+
 /* gerchbergSaxtonMultiPlane -- src/doe.js:557-626. nplanes target planes at
  * distances z[p] with target_amp / roi planes p*nx*ny (roi may be NULL) and
  * weights weight[p] (NULL = 1). per_plane_error is nplanes*iterations (row p =

@@ -312,3 +312,37 @@ def test_multiplane_batch_equals_single_designs(engine, oracle):
              "initPhase": ph[d].astype(np.float32).astype(np.float64)})
         assert np.array_equal(got["phase"][d].cpu().numpy().astype(np.float64), one["phase"])
         assert np.allclose(got["error"][d].cpu().numpy(), one["error"], rtol=1e-12, atol=0)
+
+
+def test_uneven_sizes_in_one_submission_and_graph_relaunch(engine, oracle):
+    """Size classes submitted together (direct, captured graph, graph relaunch) give
+    bitwise the results of separate per-class calls."""
+    import torch
+    from diffractiveopticalelement_b200 import batch
+    c = engine.context()
+    f = lambda a: torch.tensor(np.asarray(a, dtype=np.float32), device="cuda").contiguous()
+    spec = [(64, 3, "fourier", 12), (128, 2, "wgs-fourier", 6), (32, 4, "gs", 8), (256, 1, "wgs", 5)]
+    classes, ph0 = [], []
+    for n, B, alg, it in spec:
+        ill = oracle.disc_mask(n, n, DX, DX, 0.45 * n * DX, 2 * DX)
+        tg = [oracle.prepare_target(disc(n, n // 6 + k), ill) for k in range(B)]
+        ro = [oracle.auto_roi(disc(n, n // 6 + k), n, n) for k in range(B)]
+        p0 = f([oracle.random_phase(n, n, 70 + n + k) for k in range(B)])
+        ph0.append(p0)
+        classes.append({"nx": n, "dx": DX, "lam": LAMBDA, "z": 0.03, "algorithm": alg, "iterations": it,
+                        "illumination": f(ill), "target_amp": f(tg), "roi": f(ro), "phase": p0.clone()})
+    ref = []
+    for cl in classes:
+        kw = {k: v for k, v in cl.items() if k not in ("illumination", "target_amp", "phase", "nx", "lam")}
+        ref.append(batch.design_batch(c, cl["illumination"], cl["target_amp"], cl["phase"].clone(), nx=cl["nx"],
+                                      ny=cl["nx"], lam=cl["lam"], history=True, **kw))
+    m = batch.DesignMulti(c)
+    for mode in (0, 1, 2):
+        for cl, p0 in zip(classes, ph0):
+            cl["phase"].copy_(p0)
+        outs = m.run(classes, mode)
+        torch.cuda.synchronize()
+        for r, o in zip(ref, outs):
+            assert torch.equal(r["phase"], o["phase"]), mode
+            assert torch.equal(r["error"], o["error"]), mode
+    m.close()
