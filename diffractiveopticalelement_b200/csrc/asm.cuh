@@ -140,7 +140,7 @@ static __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
 
 // FP64 evaluation for pixels beyond the FP32 fast-path range (u > ucut):
 // exact reference classification (src/propagate.js:80-98) and FP64 phase.
-static __device__ __noinline__ float2 asm_h_slow(const AsmPlane* __restrict__ pl, const double* __restrict__ xf2,
+static __device__ __forceinline__ float2 asm_h_slow(const AsmPlane* __restrict__ pl, const double* __restrict__ xf2,
                                           const double* __restrict__ yf2, int ky, float w) {
   const AsmPlane& P = *pl;
   const double arg = (P.invL2 - *xf2) - yf2[ky];
@@ -184,7 +184,8 @@ __device__ __forceinline__ AsmCol asm_col(const AsmTables& t, int nx, int ny, in
 
 // Transfer function at bin (c.kx, ky).
 __device__ __forceinline__ float2 asm_h_col(const AsmCol& c, const AsmTables& t, int ky) {
-  const AxisBin by = c.yt[ky];
+  const float4 b4 = __ldg(reinterpret_cast<const float4*>(c.yt + ky));  // {er, ei, u, w}
+  const AxisBin by{b4.x, b4.y, b4.z, b4.w};
   const float w = c.w * by.w;
   const float u = c.u + by.u;
   const float om = fmaxf(1.f - u, 1e-3f);

@@ -120,9 +120,26 @@ extern "C" int doe_ctx_profile_read(doe_ctx* c, int max_entries, char* names, in
   return n;
 }
 
+extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value) {
+  if (!c || !key || !value) return DOE_ERR_BAD_ARG;
+  const std::string k(key);
+  if (k == "sweep_group") {
+    *value = c->tune_sweep_group;
+  } else if (k == "sweep_fused") {
+    *value = c->tune_sweep_fused;
+  } else {
+    return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
+  }
+  return DOE_OK;
+}
+
 extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) {
   if (!c || !key) return DOE_ERR_BAD_ARG;
   const std::string k(key);
+  if (k == "sweep_fused") {
+    c->tune_sweep_fused = value ? 1 : 0;
+    return DOE_OK;
+  }
   if (k == "sweep_group") {
     if (value < 0 || value > 64) return set_err(c, DOE_ERR_BAD_ARG, "sweep_group must be in [0, 64]");
     c->tune_sweep_group = (long)value;

@@ -115,6 +115,17 @@ template <class Op, class = void>
 struct HasSkip : std::false_type {};
 template <class Op>
 struct HasSkip<Op, std::void_t<decltype(std::declval<const Op&>().skip(0))>> : std::true_type {};
+// Operators may split their load: `load` issues the global reads only and
+// `finish_load(state, e, raw)` applies the pointwise factor afterwards, so that
+// every read of a thread is in flight before the first factor is evaluated (a
+// factor with a rarely taken out-of-line branch would otherwise keep the compiler
+// from hoisting the next element's read above it).
+template <class Op, class = void>
+struct HasFinishLoad : std::false_type {};
+template <class Op>
+struct HasFinishLoad<Op, std::void_t<decltype(std::declval<const Op&>().finish_load(
+                             std::declval<const typename Op::State&>(), 0, float2{}))>> : std::true_type {};
+
 template <class Op>
 __device__ __forceinline__ bool op_skip(const Op& op, int plane) {
   if constexpr (HasSkip<Op>::value) {
@@ -147,6 +158,10 @@ __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __
   if (active) {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+    if constexpr (HasFinishLoad<Op>::value) {
+#pragma unroll
+      for (int q = 0; q < RMAX; ++q) v[q] = op.finish_load(st, in_elem<P>(t, q), v[q]);
+    }
   } else {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) v[q] = make_float2(0.f, 0.f);
@@ -187,6 +202,10 @@ __global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __
   if (active) {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+    if constexpr (HasFinishLoad<Op>::value) {
+#pragma unroll
+      for (int q = 0; q < RMAX; ++q) v[q] = op.finish_load(st, in_elem<P>(t, q), v[q]);
+    }
   } else {
 #pragma unroll
     for (int q = 0; q < RMAX; ++q) v[q] = make_float2(0.f, 0.f);

@@ -149,7 +149,7 @@ struct ColAsm : NoReduce {
 
 // Column pass of a focus sweep from a resident spectrum: x H then inverse FFT.
 // Output plane p of the launch uses transfer-function table plane tp0 + p.
-struct ColSweep : NoReduce {
+struct ColSweepBase : NoReduce {
   static constexpr const char* kName = "asm_sweep_col";
   static constexpr int kStages = 1;
   static constexpr bool kInv1 = true, kInv2 = false;
@@ -165,11 +165,22 @@ struct ColSweep : NoReduce {
   __device__ __forceinline__ State init(int p, int x) const {
     return {spec + x, out + p * (long)nx * ny + x, asm_col(tab, nx, ny, tp0 + p, x)};
   }
-  __device__ __forceinline__ float2 load(const State& s, int y) const {
-    return cmul(s.spec[(long)y * nx], asm_h_col(s.h, tab, y));
-  }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
   __device__ __forceinline__ void store(const State& s, int y, float2 v, Acc&) const { s.out[(long)y * nx] = v; }
+};
+// Every spectrum read of the thread first, then the transfer function.
+struct ColSweep : ColSweepBase {
+  __device__ __forceinline__ float2 load(const State& s, int y) const { return __ldg(&s.spec[(long)y * nx]); }
+  __device__ __forceinline__ float2 finish_load(const State& s, int y, float2 v) const {
+    return cmul(v, asm_h_col(s.h, tab, y));
+  }
+};
+// Read and factor in one step per element. The autotuner keeps whichever of the
+// two formulations is faster on the device.
+struct ColSweepFused : ColSweepBase {
+  __device__ __forceinline__ float2 load(const State& s, int y) const {
+    return cmul(__ldg(&s.spec[(long)y * nx]), asm_h_col(s.h, tab, y));
+  }
 };
 
 // Inverse row pass -> FP64 split planes with 1/(nx ny).

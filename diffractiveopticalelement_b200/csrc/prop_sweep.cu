@@ -62,7 +62,9 @@ struct SweepPipe {
         float2* w = wbuf + (g % NBUF) * (long)G * pe;
         if (g >= NBUF) DOE_CUDA(c, cudaStreamWaitEvent(c->stream, ev_row(g - NBUF), 0));
         DOE_TRY(with_col(c, ny, kTuneSweep, [&](auto S) {
-          return launch_col<decltype(S)>(c, ColSweep{{}, spec, w, tab, nx, ny, g0}, gn, nx);
+          const ColSweepBase b{{}, spec, w, tab, nx, ny, g0};
+          if (c->tune_sweep_fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, gn, nx);
+          return launch_col<decltype(S)>(c, ColSweep{b}, gn, nx);
         }));
         DOE_CUDA(c, cudaEventRecord(ev_col(g), c->stream));
         DOE_CUDA(c, cudaStreamWaitEvent(c->aux, ev_col(g), 0));
@@ -222,6 +224,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
   const int lx = ilog2i(nx), ly = ilog2i(ny);
   int pick[4] = {0, 0, 0, 0};
   const int nrow = row_variant_count(nx), ncol = col_variant_count(ny);
+  float best_fused[2] = {1e30f, 1e30f};  // sweep column pass, per formulation
   for (int kind : {(int)kTuneFft, (int)kTuneSweep}) {
     float best = 1e30f;
     for (int v = 0; v < nrow; ++v) {
@@ -239,21 +242,31 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     }
     c->tune_row[kind][lx] = (unsigned char)pick[kind == kTuneFft ? 0 : 2];
     best = 1e30f;
+    int best_f = 0;
     for (int v = 0; v < ncol; ++v) {
       c->tune_col[kind][ly] = (unsigned char)v;
-      float ms;
-      DOE_TRY(time_variant(c, [&]() {
-        return with_col(c, ny, kind, [&](auto S) {
-          if (kind == kTuneSweep) return launch_col<decltype(S)>(c, ColSweep{{}, spec, w, tab, nx, ny, 0}, planes, nx);
-          return launch_col<decltype(S)>(c, ColC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, nx);
-        });
-      }, &ms));
-      if (ms < best) {
-        best = ms;
-        pick[kind == kTuneFft ? 1 : 3] = v;
+      for (int fused = 0; fused < (kind == kTuneSweep ? 2 : 1); ++fused) {
+        float ms;
+        DOE_TRY(time_variant(c, [&]() {
+          return with_col(c, ny, kind, [&](auto S) {
+            if (kind == kTuneSweep) {
+              const ColSweepBase b{{}, spec, w, tab, nx, ny, 0};
+              if (fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, planes, nx);
+              return launch_col<decltype(S)>(c, ColSweep{b}, planes, nx);
+            }
+            return launch_col<decltype(S)>(c, ColC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, nx);
+          });
+        }, &ms));
+        if (kind == kTuneSweep) best_fused[fused] = std::min(best_fused[fused], ms);
+        if (ms < best) {
+          best = ms;
+          best_f = fused;
+          pick[kind == kTuneFft ? 1 : 3] = v;
+        }
       }
     }
     c->tune_col[kind][ly] = (unsigned char)pick[kind == kTuneFft ? 1 : 3];
+    if (kind == kTuneSweep) c->tune_sweep_fused = best_f;
   }
   // planes per launch pair of the pipelined sweep: time one 64-distance field
   {

@@ -71,9 +71,13 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
                          double* total_ms, unsigned long long* count);
 
 /* Tuning knobs (engine-only): "sweep_group" = planes per focus-sweep launch pair
- * (0 = sized from the L2 cache); "fft_row", "fft_col", "sweep_row", "sweep_col",
- * "design_row", "design_col" = (log2(n) << 8) | shape variant for that pass. */
+ * (0 = sized from the L2 cache); "sweep_fused" = 1 to read and multiply per
+ * element in the sweep column pass (0: all reads first); "fft_row", "fft_col",
+ * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
+ * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
+/* Current value of "sweep_group" or "sweep_fused". */
+int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for
  * the plain FFT and focus-sweep passes, then times the pipelined sweep for
