@@ -171,9 +171,9 @@ def main_wgs(args, ctx, device, rank, world, local):
     sampler = ClockSampler(local)
     steps = max(1, args.steps if args.steps != 20 else 3)
     sampler.start()
-    r = run_wgs(ctx, device, args.designs, max(args.warmup, 3), steps, goal=0.01)
+    r = run_wgs(ctx, device, args.designs, max(args.warmup, 3), steps, goal=0.01, rank=rank)
     clocks = sampler.stop()
-    fixed = run_wgs(ctx, device, args.designs, 1, 1)
+    fixed = run_wgs(ctx, device, args.designs, 1, 1, rank=rank)
     ms = r["ms_per_step"]
     reached = r["reached"]
     if world > 1:
@@ -658,7 +658,7 @@ def wgs_cpu_baseline(n_designs=None, iters=WGS_ITERS, goal=0.01):
                       f"restatement of weightedGerchbergSaxton (no JS runtime on this box)"}
 
 
-def run_wgs(ctx, device, n_designs, warmup, steps, goal=0.0, iters=WGS_ITERS):
+def run_wgs(ctx, device, n_designs, warmup, steps, goal=0.0, iters=WGS_ITERS, rank=0):
     """Batched image-plane WGS: designs/s, screen RMSE of every design, kernel split.
 
     goal > 0: every design stops at the first iteration whose screen RMSE is <= goal
@@ -666,7 +666,7 @@ def run_wgs(ctx, device, n_designs, warmup, steps, goal=0.0, iters=WGS_ITERS):
     import torch
     from diffractiveopticalelement_b200 import batch
     L = ctx.lib
-    ill, irr, roi, tgt, ph = wgs_inputs(n_designs)
+    ill, irr, roi, tgt, ph = wgs_inputs(n_designs, seed0=1 + rank * n_designs)  # rank r: its own designs
     f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
     d_ill = f32(ill)
     d_tgt, d_roi, d_irr, d_ph0 = f32(tgt), f32(roi), f32(irr), f32(ph)

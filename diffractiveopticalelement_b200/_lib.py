@@ -134,6 +134,8 @@ def _declare(L):
         "doe_surrogate_forward": (i, [_vp, i, _vp, _vp, _vp]),
         "doe_surrogate_backward": (i, [_vp, _vp]),
         "doe_surrogate_zero_grad": (i, [_vp]),
+        "doe_surrogate_grads_dev": (i, [_vp, _vp]),
+        "doe_surrogate_set_grads_dev": (i, [_vp, _vp]),
         "doe_surrogate_adam": (i, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
         "doe_multiplane": (i, [ctxp, i, i, d, d, d, _dp, i, _dp, _dp, _dp, _dp, i, _dp, _dp, _dp, _dp, _dp]),
         "doe_autotune": (i, [ctxp, i, i, d, d, d, d, C.POINTER(C.c_int)]),

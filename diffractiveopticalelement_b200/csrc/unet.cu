@@ -627,6 +627,19 @@ extern "C" int doe_surrogate_backward(doe_surrogate* s, const float* d_dphase) {
   return DOE_OK;
 }
 
+// Device copies of the FP32 gradient buffer, for data-parallel training
+// (all-reduce between backward and Adam).
+extern "C" int doe_surrogate_grads_dev(doe_surrogate* s, float* d_out) {
+  if (!s || !d_out) return DOE_ERR_BAD_ARG;
+  DOE_CUDA(s->c, cudaMemcpyAsync(d_out, s->g, sizeof(float) * s->nparam, cudaMemcpyDeviceToDevice, s->c->stream));
+  return DOE_OK;
+}
+extern "C" int doe_surrogate_set_grads_dev(doe_surrogate* s, const float* d_in) {
+  if (!s || !d_in) return DOE_ERR_BAD_ARG;
+  DOE_CUDA(s->c, cudaMemcpyAsync(s->g, d_in, sizeof(float) * s->nparam, cudaMemcpyDeviceToDevice, s->c->stream));
+  return DOE_OK;
+}
+
 extern "C" int doe_surrogate_zero_grad(doe_surrogate* s) {
   if (!s) return DOE_ERR_BAD_ARG;
   DOE_CUDA(s->c, cudaMemsetAsync(s->g, 0, sizeof(float) * s->nparam, s->c->stream));

@@ -91,6 +91,19 @@ class Surrogate:
         with _Ordered(self.ctx):
             self.ctx.check(self.ctx.lib.doe_surrogate_backward(self.h, d.data_ptr()))
 
+    def allreduce_gradients(self, world, group=None):
+        """Average the accumulated gradients over `world` data-parallel ranks (NCCL)."""
+        if world <= 1:
+            return
+        torch = _torch()
+        from .sharding import allreduce_mean_
+        buf = torch.empty(self.count, dtype=torch.float32, device="cuda")
+        with _Ordered(self.ctx):
+            self.ctx.check(self.ctx.lib.doe_surrogate_grads_dev(self.h, buf.data_ptr()))
+        allreduce_mean_(buf, world, group)
+        with _Ordered(self.ctx):
+            self.ctx.check(self.ctx.lib.doe_surrogate_set_grads_dev(self.h, buf.data_ptr()))
+
     def zero_grad(self):
         with _Ordered(self.ctx):
             self.ctx.check(self.ctx.lib.doe_surrogate_zero_grad(self.h))
@@ -198,8 +211,11 @@ def training_targets(n, count, seed0, kinds=("rectangles", "spots", "smooth")):
 
 
 def train(model, irr_all, roi_all, illumination, target_amp_all, *, dx, lam, z, steps, batch, lr=1e-3,
-          loss="physics", target_phase_all=None, seed=0, log_every=0, lr_final=None):
-    """Adam training on device-resident sets (CUDA float32 [N, n*n]); returns the loss history."""
+          loss="physics", target_phase_all=None, seed=0, log_every=0, lr_final=None, world=1, group=None):
+    """Adam training on device-resident sets (CUDA float32 [N, n*n]); returns the loss history.
+
+    With world > 1 every rank draws its own batches (seed + rank offsets are the
+    caller's) and the gradients are averaged over ranks before each Adam step."""
     torch = _torch()
     gen = torch.Generator(device="cpu").manual_seed(seed)
     N = irr_all.shape[0]
@@ -217,6 +233,7 @@ def train(model, irr_all, roi_all, illumination, target_amp_all, *, dx, lam, z, 
         else:
             lval, g = supervised_grad(model.ctx, ph, target_phase_all[idx].contiguous())
         model.backward(g)
+        model.allreduce_gradients(world, group)
         rate = lr if lr_final is None else lr * (lr_final / lr) ** (step / max(1, steps - 1))
         model.adam(rate)
         if log_every and (step % log_every == 0 or step == steps - 1):

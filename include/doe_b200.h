@@ -335,6 +335,10 @@ int doe_surrogate_forward(doe_surrogate* s, int batch, const float* d_irr, const
  * accumulates the parameter gradients */
 int doe_surrogate_backward(doe_surrogate* s, const float* d_dphase);
 int doe_surrogate_zero_grad(doe_surrogate* s);
+/* device copies of the FP32 gradient buffer (param_count floats), for the
+ * all-reduce of data-parallel training between backward and Adam */
+int doe_surrogate_grads_dev(doe_surrogate* s, float* d_out);
+int doe_surrogate_set_grads_dev(doe_surrogate* s, const float* d_in);
 /* Adam with decoupled weight decay on grad * grad_scale; zeroes the gradients */
 int doe_surrogate_adam(doe_surrogate* s, float lr, float beta1, float beta2, float eps,
                        float weight_decay, float grad_scale);
