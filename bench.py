@@ -892,8 +892,12 @@ def main():
         bytes_per_launch = planes_per_launch * NX * NY * 16
         avg_s = tot_ms / cnt / 1000.0
         achieved = bytes_per_launch / avg_s / 1e9
+        # DRAM bytes of one full-size sweep column launch (64 planes), ncu capture in
+        # profiles/asm_sweep_col_1024.md; other kernels have no full-size capture
+        traffic = 494.03e6 * planes_per_launch / 64 if name == "asm_sweep_col" else None
         roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                    "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch",
                     "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6,
                     "launches": cnt,
                     "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()}}
