@@ -887,9 +887,13 @@ def main():
     roofline = None
     if dom:
         name, (tot_ms, cnt) = dom
-        # column pass: read spectrum + write intermediate; row pass: read intermediate + write output
+        # column pass: the spectrum once per launch + every intermediate plane written
+        # (8 B/px each); row pass: read intermediate + write output (16 B/px per plane)
         planes_per_launch = nfields * NZ / cnt
-        bytes_per_launch = planes_per_launch * NX * NY * 16
+        if name == "asm_sweep_col":
+            bytes_per_launch = (planes_per_launch + 1) * NX * NY * 8
+        else:
+            bytes_per_launch = planes_per_launch * NX * NY * 16
         avg_s = tot_ms / cnt / 1000.0
         achieved = bytes_per_launch / avg_s / 1e9
         # DRAM bytes of one full-size sweep column launch (64 planes), ncu capture in
