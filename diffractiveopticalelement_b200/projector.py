@@ -133,6 +133,12 @@ def makeTarget(kind, nx, ny, opts=None):
     return {"irradiance": irr, "roi": roi, "name": name, "grid": grid}
 
 
+# field order of doe_screen_metrics_full (the reference's screenMetrics keys)
+SCREEN_METRIC_KEYS = ["efficiency", "fluxFraction", "uniformity", "spotUniformity", "flatness", "contrast", "rmse",
+                      "fidelity", "correlation", "ssim", "snr", "zeroOrder", "rmsRadius", "meanIntensity",
+                      "peakIntensity", "powerInSignal", "powerAtScreen", "powerIncident"]
+
+
 class ProjectorSystem:
     """src/projector.js:345-718."""
 
@@ -213,24 +219,34 @@ class ProjectorSystem:
         return out
 
     def screenMetrics(self, field, opts=None):
-        """Radiometric subset of src/projector.js:554-614 (GPU FP64 reductions)."""
+        """src/projector.js:554-614: every field, from three FP64 passes on the GPU
+        (doe_screen_metrics_full). The zero-order leak is measured on the element
+        field illumination * exp(i phase), phase = opts["phase"] or the design's."""
         opts = opts or {}
         tgt = opts.get("target") or self.target
         roi = opts.get("roi")
         mask = tgt["roi"] if roi is None else roi
-        out = np.zeros(6)
+        phase = opts.get("phase")
+        if phase is None:
+            if self.result is None:
+                raise ValueError("ProjectorSystem.screenMetrics: call design() first (or pass {phase})")
+            phase = self.result["phase"]
+        ill = self.result["illumination"] if self.result is not None else self.illumination()
+        grid = tgt.get("grid")
+        out = np.zeros(18)
         c = self.ctx or _lib.context()
-        c.check(c.lib.doe_screen_metrics(c.h, _lib.dp(field.re), _lib.dp(field.im), field.nx, field.ny, field.dx,
-                                         field.dy, _lib.dp(_lib.f64(tgt["irradiance"])),
-                                         _lib.dp(None if mask is None else _lib.f64(mask)),
-                                         _lib.dp(_lib.f64(self.illumination())), self.dx, self.dy, _lib.dp(out)))
-        rmse = float(out[0])
-        return {"rmse": rmse, "efficiency": float(out[1]), "fluxFraction": float(out[2]),
-                "powerInSignal": float(out[3]), "powerAtScreen": float(out[4]), "powerIncident": float(out[5]),
-                "snr": 20 * math.log10(1 / rmse) if rmse > 0 else math.inf}
+        c.check(c.lib.doe_screen_metrics_full(
+            c.h, _lib.dp(field.re), _lib.dp(field.im), field.nx, field.ny, field.dx, field.dy,
+            _lib.dp(_lib.f64(tgt["irradiance"])), _lib.dp(None if mask is None else _lib.f64(mask)),
+            _lib.dp(_lib.f64(ill)), _lib.dp(_lib.f64(phase)), self.dx, self.dy,
+            int(grid["cols"]) if grid else 0, int(grid["rows"]) if grid else 0, _lib.dp(out)))
+        m = dict(zip(SCREEN_METRIC_KEYS, (float(v) for v in out)))
+        if not grid:
+            m["spotUniformity"] = None
+        return m
 
     def defocusCurve(self, opts=None):
-        """src/projector.js:622-642 (radiometric fields)."""
+        """src/projector.js:622-642."""
         opts = opts or {}
         points, span = opts.get("points", 21), opts.get("span", 0.6)
         z0, z1 = self.z * (1 - span), self.z * (1 + span)
@@ -238,7 +254,9 @@ class ProjectorSystem:
         for i in range(points):
             z = z0 + ((z1 - z0) * i) / (points - 1)
             m = self.screenMetrics(self.simulate({"z": z, "pad": opts.get("pad", 2), "mode": opts.get("mode")}))
-            out.append({"z": z, "zMm": z * 1e3, "rmse": m["rmse"], "efficiency": m["efficiency"]})
+            out.append({"z": z, "zMm": z * 1e3, "fidelity": m["fidelity"], "correlation": m["correlation"],
+                        "ssim": m["ssim"], "rmse": m["rmse"], "efficiency": m["efficiency"],
+                        "uniformity": m["uniformity"]})
         return out
 
     def focusStack(self, opts=None):

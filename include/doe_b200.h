@@ -288,6 +288,17 @@ int doe_screen_metrics(doe_ctx* ctx, const double* re, const double* im, int nx,
                        double sdx, double sdy, const double* target_irr, const double* roi,
                        const double* illumination, double dx, double dy, double* out);
 
+/* ProjectorSystem.screenMetrics, every field -- src/projector.js:554-614 with
+ * src/metrics.js:37-321: out[18] = {efficiency, fluxFraction, uniformity,
+ * spotUniformity (NaN unless grid_cols, grid_rows > 0), flatness, contrast, rmse,
+ * fidelity, correlation, ssim (8x8 windows, target-weighted), snr, zeroOrder (of
+ * the element field illumination * exp(i phase)), rmsRadius, meanIntensity,
+ * peakIntensity, powerInSignal, powerAtScreen, powerIncident}. roi may be NULL. */
+int doe_screen_metrics_full(doe_ctx* ctx, const double* re, const double* im, int nx, int ny,
+                            double sdx, double sdy, const double* target_irr, const double* roi,
+                            const double* illumination, const double* phase, double dx, double dy,
+                            int grid_cols, int grid_rows, double* out);
+
 /* Batched screen metrics of B device-resident screens given by their amplitudes
  * (FP32 [B][nx*ny]); target/roi/illumination use the given design strides (0 =
  * shared). out is a device array [B][6] in the order of doe_screen_metrics.

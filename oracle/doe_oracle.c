@@ -921,6 +921,212 @@ void orc_screen_metrics(const double* fre, const double* fim, int nx, int ny, do
   free(tgt);
 }
 
+/* ---------------------------------------------------------------- full screenMetrics */
+/* src/metrics.js:37-67 regionStats -> {n, mean, min, max, std, uniformity, flatness, cv} */
+static void region_stats(const double* plane, const double* mask, long n, double threshold, double* o) {
+  long cnt = 0;
+  double sum = 0, sumSq = 0, mn = INFINITY, mx = -INFINITY;
+  for (long k = 0; k < n; k++) {
+    if (mask && mask[k] <= 0) continue;
+    double v = plane[k];
+    if (v <= threshold) continue;
+    cnt++;
+    sum += v;
+    sumSq += v * v;
+    if (v < mn) mn = v;
+    if (v > mx) mx = v;
+  }
+  if (cnt == 0) {
+    for (int i = 0; i < 8; i++) o[i] = 0;
+    return;
+  }
+  double mean = sum / cnt;
+  double var = fmax(0, sumSq / cnt - mean * mean);
+  double sd = sqrt(var);
+  o[0] = (double)cnt;
+  o[1] = mean;
+  o[2] = mn;
+  o[3] = mx;
+  o[4] = sd;
+  o[5] = mx + mn > 0 ? 1 - (mx - mn) / (mx + mn) : 1;
+  o[6] = mean > 0 ? 1 - sd / mean : 1;
+  o[7] = mean > 0 ? sd / mean : 0;
+}
+
+/* src/metrics.js:87-118 correlation (two passes) */
+static double correlation(const double* p, const double* t, const double* mask, long n) {
+  double sp = 0, st = 0;
+  long cnt = 0;
+  for (long k = 0; k < n; k++) {
+    if (mask && mask[k] <= 0) continue;
+    sp += p[k];
+    st += t[k];
+    cnt++;
+  }
+  if (cnt == 0) return 0;
+  double mp = sp / cnt, mt = st / cnt, cov = 0, vp = 0, vt = 0;
+  for (long k = 0; k < n; k++) {
+    if (mask && mask[k] <= 0) continue;
+    double dp = p[k] - mp, dt = t[k] - mt;
+    cov += dp * dt;
+    vp += dp * dp;
+    vt += dt * dt;
+  }
+  return vp > 0 && vt > 0 ? cov / sqrt(vp * vt) : 0;
+}
+
+/* src/metrics.js:198-259 ssim, window 8, dataRange from the peaks, weight 'target' */
+static double ssim_target(const double* p, const double* t, int nx, int ny, int window) {
+  long n = (long)nx * ny;
+  double mx = 0;
+  for (long k = 0; k < n; k++) {
+    if (p[k] > mx) mx = p[k];
+    if (t[k] > mx) mx = t[k];
+  }
+  double L = mx > 0 ? mx : 1;
+  double C1 = 0.01 * L * (0.01 * L), C2 = 0.03 * L * (0.03 * L);
+  double total = 0, wsum = 0;
+  for (int wy = 0; wy + window <= ny; wy += window) {
+    for (int wx = 0; wx + window <= nx; wx += window) {
+      double sp = 0, st = 0, spp = 0, stt = 0, spt = 0;
+      double w2 = (double)window * window;
+      for (int j = 0; j < window; j++) {
+        for (int i = 0; i < window; i++) {
+          long k = wx + i + (long)(wy + j) * nx;
+          sp += p[k];
+          st += t[k];
+          spp += p[k] * p[k];
+          stt += t[k] * t[k];
+          spt += p[k] * t[k];
+        }
+      }
+      double mp = sp / w2, mt = st / w2;
+      double vp = fabs(spp / w2 - mp * mp), vt = fabs(stt / w2 - mt * mt);
+      double cpt = spt / w2 - mp * mt;
+      double num = (2 * mp * mt + C1) * (2 * cpt + C2);
+      double den = (mp * mp + mt * mt + C1) * (vp + vt + C2);
+      double wt = st / w2;
+      total += (den != 0 ? num / den : 0) * wt;
+      wsum += wt;
+    }
+  }
+  return wsum > 0 ? total / wsum : 0;
+}
+
+/* src/metrics.js:284-321 spotUniformity (minPeak 0.05) -> uniformity */
+static double spot_uniformity(const double* plane, int nx, int ny, int cols, int rows) {
+  long n = (long)nx * ny;
+  double* cells = (double*)calloc((size_t)cols * rows, sizeof(double));
+  double peak = 0;
+  for (long k = 0; k < n; k++)
+    if (plane[k] > peak) peak = plane[k];
+  double cut = 0.05 * peak;
+  for (int j = 0; j < ny; j++) {
+    int cj = (int)fmin(rows - 1, floor(((double)j / ny) * rows));
+    for (int i = 0; i < nx; i++) {
+      int ci = (int)fmin(cols - 1, floor(((double)i / nx) * cols));
+      double v = plane[i + (long)j * nx];
+      if (v >= cut) cells[ci + cj * cols] += v;
+    }
+  }
+  double mn = INFINITY, mx = 0;
+  int cnt = 0;
+  for (int c = 0; c < cols * rows; c++) {
+    if (cells[c] <= 0) continue;
+    mn = fmin(mn, cells[c]);
+    mx = fmax(mx, cells[c]);
+    cnt++;
+  }
+  free(cells);
+  if (cnt == 0) return 0;
+  return mx + mn > 0 ? (2 * mn) / (mx + mn) : 1;
+}
+
+/* src/projector.js:554-614 screenMetrics (all fields; spot uniformity when
+ * grid_cols > 0) with src/metrics.js:145-157 zeroOrderFraction of the element
+ * field illumination * exp(i phase) and :164-185 rmsRadius. out[18] in the
+ * order of the engine's doe_screen_metrics_full. */
+void orc_screen_metrics_full(const double* fre, const double* fim, int nx, int ny, double sdx,
+                             double sdy, const double* target_irr, const double* roi,
+                             const double* illumination, const double* phase, double dx, double dy,
+                             int grid_cols, int grid_rows, double* out) {
+  long n = (long)nx * ny;
+  double* irr = (double*)malloc(sizeof(double) * n);
+  double* tgt = (double*)malloc(sizeof(double) * n);
+  for (long k = 0; k < n; k++) irr[k] = fre[k] * fre[k] + fim[k] * fim[k];
+  double cell = sdx * sdy;
+  memcpy(tgt, target_irr, sizeof(double) * n);
+  double spt = 0, stt = 0;
+  for (long k = 0; k < n; k++) spt += roi ? irr[k] * roi[k] : irr[k];
+  for (long k = 0; k < n; k++) stt += tgt[k];
+  double pt = spt * cell, tt = stt * cell;
+  double s = tt > 0 ? pt / tt : 0;
+  for (long k = 0; k < n; k++) tgt[k] *= s;
+  double prov[8], st8[8];
+  region_stats(irr, roi, n, 0.0, prov);
+  region_stats(irr, roi, n, 0.1 * prov[3], st8);
+  double spots = grid_cols > 0 ? spot_uniformity(irr, nx, ny, grid_cols, grid_rows) : NAN;
+  double sinc = 0;
+  for (long k = 0; k < n; k++) sinc += illumination[k];
+  double incident = sinc * dx * dy;
+  double stot = 0;
+  for (long k = 0; k < n; k++) stot += irr[k];
+  double total = stot * cell, inSignal = spt * cell;
+  double num = 0, den = 0;
+  for (long k = 0; k < n; k++) {
+    double m = roi ? roi[k] : 1;
+    if (m <= 0) continue;
+    double d = irr[k] - tgt[k];
+    num += d * d;
+    den += tgt[k] * tgt[k];
+  }
+  double rms = den > 0 ? sqrt(num / den) : 0;
+  double corr = correlation(irr, tgt, roi, n);
+  double ss = ssim_target(irr, tgt, nx, ny, 8);
+  /* rmsRadius(irr, nx, sdx, 0, 0, sdy) */
+  double p = 0, sx = 0, sy = 0;
+  for (int j = 0; j < ny; j++) {
+    double y = (j - ny / 2.0) * sdy;
+    for (int i = 0; i < nx; i++) {
+      double x = (i - nx / 2.0) * sdx;
+      double v = irr[i + (long)j * nx];
+      p += v;
+      sx += v * x * x;
+      sy += v * y * y;
+    }
+  }
+  double rr = p == 0 ? 0 : hypot(sqrt(sx / p), sqrt(sy / p));
+  /* zeroOrderFraction of A exp(i phase) (src/field.js:168-179 setAmplitudePhase) */
+  double zr = 0, zi = 0, zp = 0;
+  for (long k = 0; k < n; k++) {
+    double re = illumination[k] * cos(phase[k]), im = illumination[k] * sin(phase[k]);
+    zr += re;
+    zi += im;
+    zp += re * re + im * im;
+  }
+  double zero = zp == 0 ? 0 : (zr * zr + zi * zi) / (n * zp);
+  out[0] = incident > 0 ? inSignal / incident : 0;            /* efficiency */
+  out[1] = total > 0 ? inSignal / total : 0;                  /* fluxFraction */
+  out[2] = grid_cols > 0 ? spots : st8[5];                    /* uniformity */
+  out[3] = spots;                                             /* spotUniformity (NaN: none) */
+  out[4] = st8[6];                                            /* flatness */
+  out[5] = st8[7];                                            /* contrast (cv) */
+  out[6] = rms;                                               /* rmse */
+  out[7] = (corr + 1) / 2;                                    /* fidelity */
+  out[8] = corr;                                              /* correlation */
+  out[9] = ss;                                                /* ssim */
+  out[10] = rms > 0 ? 20 * log10(1 / rms) : INFINITY;         /* snr */
+  out[11] = zero;                                             /* zeroOrder */
+  out[12] = rr;                                               /* rmsRadius */
+  out[13] = st8[1];                                           /* meanIntensity */
+  out[14] = st8[3];                                           /* peakIntensity */
+  out[15] = inSignal;                                         /* powerInSignal */
+  out[16] = total;                                            /* powerAtScreen */
+  out[17] = incident;                                         /* powerIncident */
+  free(irr);
+  free(tgt);
+}
+
 /* src/doe.js:817-829: targetAmp = sqrt(max(0, irr)), then scaled so that
  * sum(targetAmp^2) equals sum(illumination^2), both summed sequentially. */
 void orc_prepare_target(const double* irr, const double* illumination, long n, double* out) {

@@ -126,6 +126,11 @@ void orc_auto_roi(const double* irr, int nx, int ny, double dilate, double soft,
 void orc_screen_metrics(const double* field_re, const double* field_im, int nx, int ny,
                         double sdx, double sdy, const double* target_irr, const double* roi,
                         const double* illumination, double dx, double dy, double* out);
+/* src/projector.js:554-614 with src/metrics.js (all fields), out[18] */
+void orc_screen_metrics_full(const double* field_re, const double* field_im, int nx, int ny,
+                             double sdx, double sdy, const double* target_irr, const double* roi,
+                             const double* illumination, const double* phase, double dx, double dy,
+                             int grid_cols, int grid_rows, double* out);
 
 /* src/doe.js:817-829 target amplitude and power match. */
 void orc_prepare_target(const double* irr, const double* illumination, long n, double* out);

@@ -87,6 +87,7 @@ def lib():
                                         _dp, _dp, _dp, _dp]
         L.orc_auto_roi.argtypes = [_dp, i, i, d, d, d, _dp]
         L.orc_screen_metrics.argtypes = [_dp, _dp, i, i, d, d, _dp, _dp, _dp, d, d, _dp]
+        L.orc_screen_metrics_full.argtypes = [_dp, _dp, i, i, d, d, _dp, _dp, _dp, _dp, d, d, i, i, _dp]
         L.orc_prepare_target.argtypes = [_dp, _dp, C.c_long, _dp]
         _lib = L
     return _lib
@@ -221,6 +222,24 @@ def screen_metrics(fre, fim, nx, ny, sdx, sdy, target_irr, roi, illumination, dx
     keys = ["rmse", "efficiency", "fluxFraction", "powerInSignal", "powerAtScreen",
             "powerIncident"]
     return dict(zip(keys, out.tolist()))
+
+
+FULL_METRIC_KEYS = ["efficiency", "fluxFraction", "uniformity", "spotUniformity", "flatness", "contrast", "rmse",
+                    "fidelity", "correlation", "ssim", "snr", "zeroOrder", "rmsRadius", "meanIntensity",
+                    "peakIntensity", "powerInSignal", "powerAtScreen", "powerIncident"]
+
+
+def screen_metrics_full(fre, fim, nx, ny, sdx, sdy, target_irr, roi, illumination, phase, dx, dy, grid=None):
+    """ProjectorSystem.screenMetrics, every field (src/projector.js:554-614)."""
+    out = np.empty(18)
+    gc, gr = (grid["cols"], grid["rows"]) if grid else (0, 0)
+    lib().orc_screen_metrics_full(_p(_f64(fre)), _p(_f64(fim)), nx, ny, sdx, sdy, _p(_f64(target_irr)),
+                                  _p(None if roi is None else _f64(roi)), _p(_f64(illumination)),
+                                  _p(_f64(phase)), dx, dy, gc, gr, _p(out))
+    d = dict(zip(FULL_METRIC_KEYS, out.tolist()))
+    if not grid:
+        d["spotUniformity"] = None
+    return d
 
 
 # ---------------------------------------------------------------- design loops

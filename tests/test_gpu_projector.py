@@ -43,11 +43,32 @@ def test_screen_metrics_match_oracle(engine, oracle):
     f = engine.ComplexField(n, n, 8e-6)
     f.re[:] = rng.standard_normal(n * n)
     f.im[:] = rng.standard_normal(n * n)
-    m = sys_.screenMetrics(f)
+    ph = rng.uniform(-np.pi, np.pi, n * n)
+    m = sys_.screenMetrics(f, {"phase": ph})
     o = oracle.screen_metrics(f.re, f.im, n, n, f.dx, f.dy, sys_.target["irradiance"], sys_.target["roi"],
                               sys_.illumination(), sys_.dx, sys_.dy)
     for k in ("rmse", "efficiency", "fluxFraction", "powerInSignal", "powerAtScreen", "powerIncident"):
         assert abs(m[k] / o[k] - 1) < 1e-6, k
+
+
+@pytest.mark.parametrize("kind,extra", [("disc", {}), ("dots", {"cols": 6, "rows": 5}), ("ring", {})])
+def test_full_screen_metrics_match_oracle(engine, oracle, kind, extra):
+    """Every field of screenMetrics (regionStats, correlation, SSIM, spot uniformity,
+    zero order, rms radius) against the FP64 restatement of src/metrics.js."""
+    n = 128
+    sys_ = engine.ProjectorSystem({**BASE, "target": {"kind": kind, **extra}})
+    sys_.design({"iterations": 8})
+    f = sys_.simulate()
+    m = sys_.screenMetrics(f)
+    o = oracle.screen_metrics_full(f.re, f.im, n, n, f.dx, f.dy, sys_.target["irradiance"], sys_.target["roi"],
+                                   sys_.result["illumination"], sys_.result["phase"], sys_.dx, sys_.dy,
+                                   sys_.target.get("grid"))
+    assert set(m) == set(o)
+    for k, v in o.items():
+        if v is None or not np.isfinite(v):
+            assert m[k] == v or (v is not None and not np.isfinite(m[k])), k
+        else:
+            assert abs(m[k] - v) <= 1e-9 * max(1.0, abs(v)), (k, m[k], v)
 
 
 def test_projection_conserves_energy(engine):

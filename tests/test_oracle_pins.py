@@ -322,3 +322,47 @@ def test_make_rng_matches_xorshift32(oracle):
         s ^= (s << 5) & 0xFFFFFFFF
         assert r() == s / 4294967296.0
     assert oracle.Rng(0)() == oracle.Rng(1)()  # `seed >>> 0 || 1`
+
+
+def test_full_screen_metrics_known_answers(oracle):
+    """src/metrics.js definitions on planes whose answers are known by construction."""
+    n, d = 64, 8e-6
+    i = np.arange(n)
+    X, Y = np.meshgrid(i, i)
+    disc = (np.hypot(X - n / 2, Y - n / 2) <= 12).astype(float).ravel()
+    ill = np.ones(n * n)
+    flat = np.zeros(n * n)
+    # a flat screen over the ROI: uniform; correlation is 0 by definition (no variance)
+    amp = np.sqrt(3.0 * disc)
+    m = oracle.screen_metrics_full(amp, np.zeros(n * n), n, n, d, d, disc, disc, ill, flat, d, d)
+    assert m["rmse"] == 0 and m["correlation"] == 0 and abs(m["ssim"] - 1) < 1e-12
+    assert m["uniformity"] == 1 and m["flatness"] == 1 and m["contrast"] == 0 and m["fidelity"] == 0.5
+    assert m["snr"] == float("inf") and m["spotUniformity"] is None
+    assert abs(m["meanIntensity"] - 3.0) < 1e-12 and abs(m["peakIntensity"] - 3.0) < 1e-12
+    # screen = 3 x a structured target: perfect fidelity
+    tg = disc * (1.5 + np.cos(X / 3.0).ravel())
+    ms = oracle.screen_metrics_full(np.sqrt(3.0 * tg), np.zeros(n * n), n, n, d, d, tg, disc, ill, flat, d, d)
+    assert ms["rmse"] < 1e-15 and abs(ms["correlation"] - 1) < 1e-12 and abs(ms["ssim"] - 1) < 1e-12
+    # flat element phase: all power in the zero order; a 0/pi checkerboard: none
+    assert abs(m["zeroOrder"] - 1) < 1e-12
+    cb = np.where((X + Y) % 2 == 0, 0.0, np.pi).ravel()
+    m2 = oracle.screen_metrics_full(amp, np.zeros(n * n), n, n, d, d, disc, disc, ill, cb, d, d)
+    assert m2["zeroOrder"] < 1e-20
+    # rms radius: two equal points at (+-a, 0) from the centre -> r = a
+    two = np.zeros((n, n))
+    two[n // 2, n // 2 - 5] = two[n // 2, n // 2 + 5] = 1.0
+    m3 = oracle.screen_metrics_full(two.ravel(), np.zeros(n * n), n, n, d, d, disc, None, ill, flat, d, d)
+    assert abs(m3["rmsRadius"] - 5 * d) < 1e-18
+    # spot cells: equal power in every lit cell -> uniformity 1
+    spots = np.zeros((n, n))
+    for a in range(4):
+        for b in range(4):
+            spots[8 + 16 * b, 8 + 16 * a] = 2.0
+    g = {"cols": 4, "rows": 4}
+    m4 = oracle.screen_metrics_full(np.sqrt(spots.ravel()), np.zeros(n * n), n, n, d, d, spots.ravel(), None, ill,
+                                    flat, d, d, g)
+    assert m4["spotUniformity"] == 1 and m4["uniformity"] == 1
+    spots[8, 8] = 1.0  # one cell at half power -> 2 min / (max + min) = 2/3
+    m5 = oracle.screen_metrics_full(np.sqrt(spots.ravel()), np.zeros(n * n), n, n, d, d, spots.ravel(), None, ill,
+                                    flat, d, d, g)
+    assert abs(m5["spotUniformity"] - 2 / 3) < 1e-12
