@@ -842,8 +842,10 @@ def main():
     ctx.check(L.doe_autotune(ctx.h, NX, NY, DX, DX, 532e-9, 0.03, chosen))
     fused = C.c_longlong(0)
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_fused", C.byref(fused)))
+    graph = C.c_longlong(0)
+    ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_graph", C.byref(graph)))
     tuned = {"fft_row": chosen[0], "fft_col": chosen[1], "sweep_row": chosen[2], "sweep_col": chosen[3],
-             "sweep_group": chosen[4], "sweep_fused_load": int(fused.value)}
+             "sweep_group": chosen[4], "sweep_fused_load": int(fused.value), "sweep_graph": int(graph.value)}
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         step()

@@ -58,6 +58,7 @@ extern "C" void doe_ctx_destroy(doe_ctx* c) {
   }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   for (auto e : c->sync_ev) cudaEventDestroy(e);
+  if (c->sweep_exec) cudaGraphExecDestroy(c->sweep_exec);
   if (c->aux) {
     cudaStreamSynchronize(c->aux);
     cudaStreamDestroy(c->aux);
@@ -127,6 +128,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_group;
   } else if (k == "sweep_fused") {
     *value = c->tune_sweep_fused;
+  } else if (k == "sweep_graph") {
+    *value = c->tune_sweep_graph;
   } else {
     return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
   }
@@ -138,6 +141,10 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   const std::string k(key);
   if (k == "sweep_fused") {
     c->tune_sweep_fused = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "sweep_graph") {
+    c->tune_sweep_graph = value ? 1 : 0;
     return DOE_OK;
   }
   if (k == "sweep_group") {

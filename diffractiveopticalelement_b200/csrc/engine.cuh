@@ -45,6 +45,9 @@ struct doe_ctx {
   cudaStream_t aux = nullptr;          // second stream for pipelined passes
   std::vector<cudaEvent_t> sync_ev;    // events ordering the two streams
   long tune_sweep_group = 0;           // planes per sweep launch pair (0 = from L2 size)
+  int tune_sweep_graph = 1;            // replay repeated device sweeps from a captured CUDA graph
+  cudaGraphExec_t sweep_exec = nullptr;  // graph of the last repeated device sweep
+  unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
   unsigned char tune_row[4][16] = {};  // chosen row-shape variant per [kind][log2 N]
   unsigned char tune_col[4][16] = {};  // chosen column-shape variant per [kind][log2 N]

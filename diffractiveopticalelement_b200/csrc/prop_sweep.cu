@@ -138,6 +138,27 @@ extern "C" int doe_asm_sweep(doe_ctx* c, const double* re, const double* im, int
   return DOE_OK;
 }
 
+namespace {
+// FNV-1a over the bytes of a value sequence (the identity of a repeated sweep).
+struct Fnv {
+  unsigned long long h = 1469598103934665603ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  }
+  template <class T>
+  void val(const T& v) { add(&v, sizeof(v)); }
+};
+
+int sweep_dev_body(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny, double dx, double dy,
+                   const double* lambda, const double* z, int nz, int band_limit, int evanescent, double soft_edge,
+                   void* d_out);
+}  // namespace
+
+// Device sweeps repeated with identical arguments (same pointers, geometry and
+// distances, same tuning) are replayed from a CUDA graph captured on the second
+// such call: the ~2 launches per plane group and their stream joins then cost one
+// graph launch, which lets the autotuner choose small, L2-resident plane groups.
 extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny, double dx, double dy,
                                  const double* lambda, const double* z, int nz, int band_limit, int evanescent,
                                  double soft_edge, void* d_out) {
@@ -145,6 +166,63 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
   DOE_TRY(check_grid(c, nx, ny, "focusSweep"));
   if (!d_fields || !lambda || !z || !d_out || nfields < 0 || nz < 0)
     return set_err(c, DOE_ERR_BAD_ARG, "focusSweep: bad argument");
+  if (!c->tune_sweep_graph || c->prof_on)
+    return sweep_dev_body(c, d_fields, nfields, nx, ny, dx, dy, lambda, z, nz, band_limit, evanescent, soft_edge,
+                          d_out);
+  Fnv k;
+  k.val(d_fields);
+  k.val(d_out);
+  for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused}) k.val(v);
+  for (double v : {dx, dy, soft_edge}) k.val(v);
+  k.val(c->tune_sweep_group);
+  k.add(c->tune_row, sizeof(c->tune_row));
+  k.add(c->tune_col, sizeof(c->tune_col));
+  k.add(lambda, sizeof(double) * (size_t)nfields);
+  k.add(z, sizeof(double) * (size_t)nfields * nz);
+  if (c->sweep_exec && k.h == c->sweep_key) {
+    DOE_CUDA(c, cudaGraphLaunch(c->sweep_exec, c->stream));
+    c->launches += c->sweep_launches;
+    return DOE_OK;
+  }
+  if (k.h != c->sweep_pending) {  // first sighting: run directly (sizes the scratch)
+    c->sweep_pending = k.h;
+    return sweep_dev_body(c, d_fields, nfields, nx, ny, dx, dy, lambda, z, nz, band_limit, evanescent, soft_edge,
+                          d_out);
+  }
+  if (c->sweep_exec) {
+    cudaGraphExecDestroy(c->sweep_exec);
+    c->sweep_exec = nullptr;
+  }
+  const unsigned long long n0 = c->launches;
+  DOE_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  const int rc = sweep_dev_body(c, d_fields, nfields, nx, ny, dx, dy, lambda, z, nz, band_limit, evanescent,
+                                soft_edge, d_out);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  const unsigned long long used = c->launches - n0;
+  c->launches = n0;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_err(c, DOE_ERR_CUDA, "focusSweep: capture failed: %s", cudaGetErrorString(e));
+  const cudaError_t e2 = cudaGraphInstantiate(&c->sweep_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) {
+    c->sweep_exec = nullptr;
+    return set_err(c, DOE_ERR_CUDA, "focusSweep: graph instantiation failed: %s", cudaGetErrorString(e2));
+  }
+  c->sweep_key = k.h;
+  c->sweep_launches = used;
+  DOE_CUDA(c, cudaGraphLaunch(c->sweep_exec, c->stream));
+  c->launches += used;
+  return DOE_OK;
+}
+
+namespace {
+int sweep_dev_body(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny, double dx, double dy,
+                   const double* lambda, const double* z, int nz, int band_limit, int evanescent, double soft_edge,
+                   void* d_out) {
   const long pe = (long)nx * ny;
   void* dspec;
   DOE_TRY(ensure_slot(c, kSlotW0, pe * sizeof(float2), &dspec));
@@ -165,6 +243,7 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
   }
   return pipe.finish();
 }
+}  // namespace
 
 // ====================================================================== autotuner
 // Times every compiled shape variant of the plain FFT passes (kTuneFft) and of
@@ -174,6 +253,46 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
 // chosen[0..4] receives {fft row, fft col, sweep row, sweep col} variant indices
 // and the sweep group size.
 namespace doe {
+// Best of three launches of `launch` captured into a CUDA graph (after one direct
+// run that sizes the scratch).
+static int time_graph(doe_ctx* c, const std::function<int()>& launch, float* ms_out) {
+  DOE_TRY(launch());
+  DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+  const unsigned long long n0 = c->launches;
+  DOE_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  const int rc = launch();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  c->launches = n0;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_err(c, DOE_ERR_CUDA, "autotune: capture failed: %s", cudaGetErrorString(e));
+  cudaGraphExec_t x = nullptr;
+  const cudaError_t e2 = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) return set_err(c, DOE_ERR_CUDA, "autotune: instantiation failed: %s", cudaGetErrorString(e2));
+  cudaEvent_t a = prof_event(c), b = prof_event(c);
+  float best = 1e30f;
+  int rc2 = DOE_OK;
+  for (int rep = 0; rep < 4 && !rc2; ++rep) {
+    if (cudaEventRecord(a, c->stream) != cudaSuccess || cudaGraphLaunch(x, c->stream) != cudaSuccess ||
+        cudaEventRecord(b, c->stream) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess) {
+      rc2 = set_err(c, DOE_ERR_CUDA, "autotune: graph timing failed");
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  c->ev_pool.push_back(a);
+  c->ev_pool.push_back(b);
+  cudaGraphExecDestroy(x);
+  *ms_out = best;
+  return rc2;
+}
+
 static int time_variant(doe_ctx* c, const std::function<int()>& launch, float* ms_out) {
   cudaEvent_t a = prof_event(c), b = prof_event(c);  // timing-enabled events
   struct Give {
@@ -282,7 +401,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
       if ((size_t)G * pe * sizeof(float2) * SweepPipe::NBUF > ((size_t)1 << 31)) break;
       c->tune_sweep_group = G;
       float ms;
-      DOE_TRY(time_variant(c, [&]() {
+      DOE_TRY((c->tune_sweep_graph ? time_graph : time_variant)(c, [&]() {
         SweepPipe pipe;
         DOE_TRY(pipe.init(c, nx, ny));
         DOE_TRY(pipe.run_field(spec, dx, dy, lambda, zs.data(), nz, 1, 1, 0.02, (float2*)dout, spec, nullptr,

@@ -222,3 +222,33 @@ def test_fresnel_argument_errors(engine):
         engine.propagateFresnelFFT(f, LAMBDA, 0.0)
     g = engine.propagate(gaussian_phase_field(engine, 64, 64, 8e-6, 1), LAMBDA, 0.05, {"method": "fresnel"})
     assert g.dx == pytest.approx(LAMBDA * 0.05 / (64 * 8e-6))
+
+
+def test_repeated_device_sweep_replays_graph_bitwise(engine):
+    """A device sweep repeated with identical arguments is captured into a CUDA graph
+    on its second call and replayed afterwards; every call gives the same planes."""
+    import ctypes as C
+    import torch
+    ctx = engine.Context(0)
+    L = ctx.lib
+    n, nf, nz = 128, 3, 10
+    rng = np.random.default_rng(3)
+    fields = torch.tensor((rng.standard_normal((nf, n, n)) + 1j * rng.standard_normal((nf, n, n))).astype(np.complex64),
+                          device="cuda")
+    lam = np.array([450e-9, 532e-9, 633e-9])
+    zs = np.linspace(0.01, 0.05, nf * nz)
+    dp = C.POINTER(C.c_double)
+    outs = []
+    for graph in (0, 1, 1, 1, 1):
+        ctx.check(L.doe_ctx_set_tuning(ctx.h, b"sweep_graph", graph))
+        ctx.check(L.doe_ctx_set_tuning(ctx.h, b"sweep_group", 4))
+        out = torch.zeros((nf * nz, n, n), dtype=torch.complex64, device="cuda")
+        for _ in range(3 if graph else 1):
+            out.zero_()
+            ctx.check(L.doe_asm_sweep_dev(ctx.h, fields.data_ptr(), nf, n, n, 4e-6, 4e-6, lam.ctypes.data_as(dp),
+                                          zs.ctypes.data_as(dp), nz, 1, 1, 0.02, out.data_ptr()))
+        ctx.synchronize()
+        outs.append(out.cpu())
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+    ctx.close()
