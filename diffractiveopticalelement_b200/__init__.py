@@ -8,7 +8,7 @@ sm_100a CUDA kernels behind the C ABI in include/doe_b200.h
 from ._lib import DOEError, EngineUnavailable, Context, context, load_library
 from .fft import fft2d, fft2dOut, isPow2, nextPow2
 from .field import ComplexField, discMask, rectMask, ringMask
-from .doe import (DEFAULT_DESIGN, blurRaster, designDOE, flatPhase, fourierCgh, gerchbergSaxton,
+from .doe import (DEFAULT_DESIGN, blurRaster, designDOE, errorDiffusionQuantize, flatPhase, fourierCgh, gerchbergSaxton,
                   gerchbergSaxtonMultiPlane, illuminationProfile, kinoformLens, makeRng, prepareTargetAmp,
                   randomPhase, weightedGerchbergSaxton, wrapPhase)
 from .projector import DEFAULT_PROJECTOR, ProjectorSystem, autoRoi, makeTarget
@@ -34,7 +34,7 @@ __all__ = [
     "fresnelMinDistance", "localFrequencyLimit", "propagate", "propagateAngularSpectrum",
     "propagateAngularSpectrumInPlace", "propagateFraunhofer", "propagateFresnelFFT", "propagateFresnelFFTInverse",
     "discMask", "rectMask", "ringMask", "DEFAULT_DESIGN", "blurRaster",
-    "designDOE", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
+    "designDOE", "errorDiffusionQuantize", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
     "kinoformLens", "makeRng", "prepareTargetAmp", "randomPhase", "weightedGerchbergSaxton", "wrapPhase",
     "DEFAULT_PROJECTOR", "ProjectorSystem", "autoRoi", "makeTarget",
 ]

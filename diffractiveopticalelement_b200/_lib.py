@@ -122,6 +122,7 @@ def _declare(L):
         "doe_multiplane_dev": (i, [ctxp, C.POINTER(MultiplaneDevDesc)]),
         "doe_phase_loss_grad": (i, [ctxp, C.POINTER(PhaseLossDesc)]),
         "doe_design_multi_create": (i, [ctxp, C.POINTER(C.c_void_p)]),
+        "doe_error_diffusion": (i, [ctxp, i, C.c_longlong, i, i, i, _dp, _dp]),
         "doe_screen_metrics_full": (i, [ctxp, _dp, _dp, i, i, d, d, _dp, _dp, _dp, _dp, d, d, i, i, _dp]),
         "doe_ctx_get_tuning": (i, [ctxp, C.c_char_p, C.POINTER(C.c_longlong)]),
         "doe_design_multi_destroy": (None, [_vp]),

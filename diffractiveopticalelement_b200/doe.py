@@ -71,6 +71,23 @@ def wrapPhase(phi):
     return np.where(p <= -math.pi, p + 2 * math.pi, p)
 
 
+def errorDiffusionQuantize(phi, levels=4, opts=None, *, ctx=None):
+    """Floyd-Steinberg error-diffusion quantisation of a wrapped phase (src/doe.js:185-226).
+
+    `phi` is one phase plane or a [B, n] stack (each quantised independently in
+    one engine call); options `snake` (default True) and `wrapFirst` (True).
+    """
+    o = opts or {}
+    p = np.ascontiguousarray(phi, dtype=np.float64)
+    batch = 1 if p.ndim == 1 else p.shape[0]
+    n = p.size // batch
+    out = np.empty_like(p)
+    c = ctx or _lib.context()
+    c.check(c.lib.doe_error_diffusion(c.h, batch, n, int(levels), int(bool(o.get("snake", True))),
+                                      int(bool(o.get("wrapFirst", True))), _lib.dp(p), _lib.dp(out)))
+    return out
+
+
 def kinoformLens(nx, ny, dx, dy, lam, f):
     """Wrapped thin-lens phase -k r^2 / (2 f) (src/doe.js:147-151, src/propagate.js:395-407)."""
     k = 2 * math.pi / lam
@@ -284,8 +301,11 @@ def designDOE(cfg, *, ctx=None):
                   if algorithm == "wgs" else gerchbergSaxton(illumination, targetAmp, common, ctx=ctx))
         result["mode"] = "image-plane"
     result["algorithm"] = algorithm
-    if levels > 1:
-        raise NotImplementedError("designDOE: phase quantisation (levels > 1) is not part of this engine")
+    if levels > 1:  # src/doe.js:878-884
+        result["phaseContinuous"] = np.array(result["phase"], dtype=np.float64)
+        result["phase"] = errorDiffusionQuantize(result["phase"], levels, ctx=ctx)
+        result["levels"] = levels
+        result["quantized"] = True
     result.update({"illumination": illumination, "targetAmp": targetAmp, "roi": roi, "lambda": lam, "z": z,
                    "nx": nx, "ny": ny, "dx": dx, "dy": dy})
     return result

@@ -14,7 +14,7 @@ import math
 import numpy as np
 
 from . import _lib
-from .doe import designDOE, gerchbergSaxtonMultiPlane, illuminationProfile, makeRng
+from .doe import designDOE, errorDiffusionQuantize, gerchbergSaxtonMultiPlane, illuminationProfile, makeRng
 from .field import ComplexField
 
 DEFAULT_PROJECTOR = {
@@ -289,6 +289,9 @@ class ProjectorSystem:
         out = {**res, "illumination": illumination, "lambda": self.lam, "nx": self.nx, "ny": self.ny,
                "dx": self.dx, "dy": self.dy, "z": self.z, "mode": "multi-plane", "planes": planes,
                "target": self.target, "roi": self.target["roi"]}
+        levels = opts.get("levels", self.cfg["levels"]) or 0
+        if levels > 1:  # src/projector.js:708
+            out["phase"] = errorDiffusionQuantize(out["phase"], levels, ctx=self.ctx)
         self.result = out
         return out
 

@@ -181,6 +181,16 @@ typedef struct doe_design_result {
  * the seeded initial phase in (-pi, pi]. Host-side, needs no context. */
 int doe_random_phase(int nx, int ny, double seed, double* out);
 
+/* errorDiffusionQuantize -- src/doe.js:185-226: serpentine (snake) Floyd-Steinberg
+ * quantisation of `batch` phase planes of n samples each to `levels` levels, the
+ * error taken on the unit circle; wrap_first wraps the input into (-pi, pi] first.
+ * The grid is inferred as the reference does (nx = round(sqrt(n))); when nx does
+ * not divide n the call fails with "expected a square grid" (the reference then
+ * indexes past its array). Host FP64 arrays [batch][n]; one element per GPU
+ * thread, bitwise the FP64 scan. */
+int doe_error_diffusion(doe_ctx* ctx, int batch, long long n, int levels, int snake, int wrap_first,
+                        const double* phase, double* out);
+
 /* gerchbergSaxton / weightedGerchbergSaxton / fourierCgh on one design. */
 int doe_design(doe_ctx* ctx, const doe_design_desc* desc, doe_design_result* result);
 /* n designs sharing grid, pitch, algorithm and iterations, run as one batch. */

@@ -816,8 +816,12 @@ int orc_gs_multiplane(const double* illumination, int nplanes, const double* zs,
 }
 
 /* ------------------------------------------------------------------ */
-/* JavaScript Math.round: round half toward +infinity. */
-static double js_round(double x) { return floor(x + 0.5); }
+/* JavaScript Math.round: the nearest integer, ties toward +infinity (x - floor(x)
+ * is exact, so values just below a half do not round up as floor(x + 0.5) can). */
+static double js_round(double x) {
+  double f = floor(x);
+  return (x - f >= 0.5) ? f + 1.0 : f;
+}
 
 /* src/projector.js:262-315 */
 void orc_auto_roi(const double* irr, int nx, int ny, double dilate, double soft,
@@ -919,6 +923,54 @@ void orc_screen_metrics(const double* fre, const double* fim, int nx, int ny, do
   out[5] = incident;
   free(irr);
   free(tgt);
+}
+
+/* ---------------------------------------------------------------- quantisation */
+static double wrap1(double p) { /* src/propagate.js:410-420 */
+  double two_pi = 2 * M_PI;
+  p = fmod(p, two_pi);
+  if (p > M_PI) p -= two_pi;
+  else if (p <= -M_PI) p += two_pi;
+  return p;
+}
+
+/* src/doe.js:164-173 quantizePhase */
+void orc_quantize_phase(const double* phi, long n, int levels, double* out) {
+  double step = (2 * M_PI) / levels;
+  for (long k = 0; k < n; k++) out[k] = wrap1(js_round(phi[k] / step) * step);
+}
+
+/* src/doe.js:185-226 errorDiffusionQuantize; returns -1 for a non-square length */
+int orc_error_diffusion(const double* phi, long n, int levels, int snake, int wrap_first, double* out) {
+  long nx = lround(sqrt((double)n));
+  long ny = nx > 0 ? n / nx : 0;
+  if (nx * ny != n) return -1;
+  double* buf = (double*)malloc(sizeof(double) * n);
+  for (long k = 0; k < n; k++) buf[k] = wrap_first ? wrap1(phi[k]) : phi[k];
+  double step = (2 * M_PI) / levels, two_pi = 2 * M_PI;
+  for (long j = 0; j < ny; j++) {
+    int ltr = snake ? (j % 2 == 0) : 1;
+    long iStart = ltr ? 0 : nx - 1, iEnd = ltr ? nx : -1, iStep = ltr ? 1 : -1;
+    for (long i = iStart; i != iEnd; i += iStep) {
+      long k = i + j * nx;
+      double v = buf[k];
+      double q = js_round(v / step) * step;
+      out[k] = q;
+      double e = v - q;
+      if (e > M_PI) e -= two_pi;
+      else if (e <= -M_PI) e += two_pi;
+      const long di[4] = {1, -1, 0, 1}, dj[4] = {0, 1, 1, 1};
+      const double w[4] = {7.0 / 16, 3.0 / 16, 5.0 / 16, 1.0 / 16};
+      for (int t = 0; t < 4; t++) {
+        long ii = i + iStep * di[t], jj = j + dj[t];
+        if (ii < 0 || ii >= nx || jj < 0 || jj >= ny) continue;
+        buf[ii + jj * nx] += e * w[t];
+      }
+    }
+  }
+  for (long k = 0; k < n; k++) out[k] = wrap1(out[k]);
+  free(buf);
+  return 0;
 }
 
 /* ---------------------------------------------------------------- full screenMetrics */

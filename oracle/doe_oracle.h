@@ -123,6 +123,9 @@ void orc_auto_roi(const double* irr, int nx, int ny, double dilate, double soft,
  * src/projector.js:554-595 rmse / efficiency / fluxFraction subset of screenMetrics.
  * out = {rmse, efficiency, fluxFraction, powerInSignal, powerAtScreen, powerIncident}.
  */
+/* src/doe.js:164-173, :185-226 */
+void orc_quantize_phase(const double* phi, long n, int levels, double* out);
+int orc_error_diffusion(const double* phi, long n, int levels, int snake, int wrap_first, double* out);
 void orc_screen_metrics(const double* field_re, const double* field_im, int nx, int ny,
                         double sdx, double sdy, const double* target_irr, const double* roi,
                         const double* illumination, double dx, double dy, double* out);

@@ -87,6 +87,8 @@ def lib():
                                         _dp, _dp, _dp, _dp]
         L.orc_auto_roi.argtypes = [_dp, i, i, d, d, d, _dp]
         L.orc_screen_metrics.argtypes = [_dp, _dp, i, i, d, d, _dp, _dp, _dp, d, d, _dp]
+        L.orc_quantize_phase.argtypes = [_dp, C.c_long, i, _dp]
+        L.orc_error_diffusion.argtypes = [_dp, C.c_long, i, i, i, _dp]
         L.orc_screen_metrics_full.argtypes = [_dp, _dp, i, i, d, d, _dp, _dp, _dp, _dp, d, d, i, i, _dp]
         L.orc_prepare_target.argtypes = [_dp, _dp, C.c_long, _dp]
         _lib = L
@@ -222,6 +224,23 @@ def screen_metrics(fre, fim, nx, ny, sdx, sdy, target_irr, roi, illumination, dx
     keys = ["rmse", "efficiency", "fluxFraction", "powerInSignal", "powerAtScreen",
             "powerIncident"]
     return dict(zip(keys, out.tolist()))
+
+
+def quantize_phase(phi, levels=4):
+    """quantizePhase (src/doe.js:164-173)."""
+    p = _f64(phi)
+    out = np.empty(p.size)
+    lib().orc_quantize_phase(_p(p), p.size, levels, _p(out))
+    return out
+
+
+def error_diffusion(phi, levels=4, snake=True, wrap_first=True):
+    """errorDiffusionQuantize (src/doe.js:185-226)."""
+    p = _f64(phi)
+    out = np.empty(p.size)
+    if lib().orc_error_diffusion(_p(p), p.size, levels, int(snake), int(wrap_first), _p(out)):
+        raise ValueError("errorDiffusionQuantize: expected a square grid")
+    return out
 
 
 FULL_METRIC_KEYS = ["efficiency", "fluxFraction", "uniformity", "spotUniformity", "flatness", "contrast", "rmse",

@@ -346,3 +346,28 @@ def test_uneven_sizes_in_one_submission_and_graph_relaunch(engine, oracle):
             assert torch.equal(r["phase"], o["phase"]), mode
             assert torch.equal(r["error"], o["error"]), mode
     m.close()
+
+
+@pytest.mark.parametrize("n,levels,snake", [(64, 4, True), (128, 8, True), (32, 2, False), (1, 4, True)])
+def test_error_diffusion_matches_oracle_bitwise(engine, oracle, n, levels, snake):
+    """errorDiffusionQuantize (src/doe.js:185-226) on the GPU: bitwise the FP64 scan,
+    for one plane and for a batch of planes in one call."""
+    rng = np.random.default_rng(n + levels)
+    phis = rng.uniform(-9, 9, (3, n * n))
+    got = engine.errorDiffusionQuantize(phis, levels, {"snake": snake})
+    for b in range(3):
+        want = oracle.error_diffusion(phis[b], levels, snake=snake)
+        assert np.array_equal(got[b], want)
+        assert np.array_equal(engine.errorDiffusionQuantize(phis[b], levels, {"snake": snake}), want)
+    from diffractiveopticalelement_b200 import DOEError
+    with pytest.raises(DOEError, match="square grid"):
+        engine.errorDiffusionQuantize(np.zeros(50), 4)
+
+
+def test_design_doe_levels_quantises_like_the_reference(engine, oracle):
+    """designDOE with levels > 1 (src/doe.js:878-884): continuous phase kept, phase quantised."""
+    cfg = {"nx": 64, "ny": 64, "dx": DX, "lambda": LAMBDA, "z": 0.03, "iterations": 6, "target": disc(64, 20),
+           "levels": 8}
+    r = engine.designDOE(cfg)
+    assert r["quantized"] and r["levels"] == 8
+    assert np.array_equal(r["phase"], oracle.error_diffusion(r["phaseContinuous"], 8))

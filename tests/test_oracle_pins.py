@@ -366,3 +366,28 @@ def test_full_screen_metrics_known_answers(oracle):
     m5 = oracle.screen_metrics_full(np.sqrt(spots.ravel()), np.zeros(n * n), n, n, d, d, spots.ravel(), None, ill,
                                     flat, d, d, g)
     assert abs(m5["spotUniformity"] - 2 / 3) < 1e-12
+
+
+def test_error_diffusion_restatement(oracle):
+    """src/doe.js:185-226: levels only, the local mean phase kept better than
+    rounding (the reference's stated purpose), the square-grid requirement."""
+    n = 64
+    i = np.arange(n)
+    X, Y = np.meshgrid(i, i)
+    phi = (0.37 * X + 0.11 * Y + 0.5 * np.sin(X / 5.0)).ravel()  # smooth, wrapping ramp
+    q = oracle.error_diffusion(phi, 4)
+    step = 2 * np.pi / 4
+    k = np.round(q / step)
+    assert np.all(np.abs(q - k * step) < 1e-12) and np.all(q > -np.pi) and np.all(q <= np.pi + 1e-12)
+    # the phase of the local mean of exp(i phase) (2x2 and 8x8 cells) stays closer to
+    # the continuous one than with nearest-level rounding
+    r = oracle.quantize_phase(phi, 4)
+    for c in (2, 8):
+        cell = lambda p: np.exp(1j * p).reshape(n // c, c, n // c, c).mean(axis=(1, 3))
+        ref = cell(phi)
+        assert np.mean(np.abs(np.angle(cell(q) / ref))) < 0.8 * np.mean(np.abs(np.angle(cell(r) / ref)))
+    # identity at a quantised input (no error to diffuse beyond rounding)
+    d = oracle.error_diffusion(r, 4) - r
+    assert np.max(np.abs(np.angle(np.exp(1j * d)))) < 1e-12
+    with pytest.raises(ValueError, match="square"):
+        oracle.error_diffusion(np.zeros(50), 4)  # round(sqrt(50)) = 7 does not divide 50
