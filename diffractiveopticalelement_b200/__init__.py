@@ -11,6 +11,8 @@ from .field import ComplexField, discMask, rectMask, ringMask
 from .doe import (DEFAULT_DESIGN, blurRaster, designDOE, errorDiffusionQuantize, flatPhase, fourierCgh, gerchbergSaxton,
                   gerchbergSaxtonMultiPlane, illuminationProfile, kinoformLens, makeRng, prepareTargetAmp,
                   randomPhase, weightedGerchbergSaxton, wrapPhase)
+from .interference import (modalIntensity, partiallyCoherentModes, propagatedModalIntensity, reconstructHologram,
+                           recordHologram)
 from .projector import DEFAULT_PROJECTOR, ProjectorSystem, autoRoi, makeTarget
 from .propagate import (
     DEFAULT_WAVELENGTH,
@@ -37,4 +39,5 @@ __all__ = [
     "designDOE", "errorDiffusionQuantize", "flatPhase", "fourierCgh", "gerchbergSaxton", "gerchbergSaxtonMultiPlane", "illuminationProfile",
     "kinoformLens", "makeRng", "prepareTargetAmp", "randomPhase", "weightedGerchbergSaxton", "wrapPhase",
     "DEFAULT_PROJECTOR", "ProjectorSystem", "autoRoi", "makeTarget",
+    "modalIntensity", "partiallyCoherentModes", "propagatedModalIntensity", "reconstructHologram", "recordHologram",
 ]

@@ -123,6 +123,10 @@ def _declare(L):
         "doe_phase_loss_grad": (i, [ctxp, C.POINTER(PhaseLossDesc)]),
         "doe_design_multi_create": (i, [ctxp, C.POINTER(C.c_void_p)]),
         "doe_error_diffusion": (i, [ctxp, i, C.c_longlong, i, i, i, _dp, _dp]),
+        "doe_hologram_record": (i, [ctxp, _dp, _dp, _dp, _dp, C.c_longlong, i, i, _dp, _dp, _dp, _dp, _dp]),
+        "doe_hologram_reconstruct": (i, [ctxp, _dp, _dp, _dp, _dp, i, i, d, d, d, d, i, i, d] + [_dp] * 6),
+        "doe_modal_intensity": (i, [ctxp, i, _dp, _dp, i, i, _dp, d, d, d, d, i, i, d, _dp]),
+        "doe_partially_coherent_modes": (i, [ctxp, i, i, d, d, i, d, d, d, _dp, _dp]),
         "doe_screen_metrics_full": (i, [ctxp, _dp, _dp, i, i, d, d, _dp, _dp, _dp, _dp, d, d, i, i, _dp]),
         "doe_ctx_get_tuning": (i, [ctxp, C.c_char_p, C.POINTER(C.c_longlong)]),
         "doe_design_multi_destroy": (None, [_vp]),

@@ -63,6 +63,15 @@ struct DefCol {
   using type = ColShape<P, C>;
 };
 
+// 2048-point columns: radix 32-2-32 with 4 columns per CTA (256 threads, 128
+// registers, no spills) beats the default 16-8-16 plan with 512-thread CTAs in
+// the design loops' two-transform column passes on B200; rows keep the default
+// (their fused operators spill at RMAX 32).
+template <>
+struct DefCol<2048> {
+  using type = ColShape<FftPlan<2048, 3, 32, 2, 32>, 4>;
+};
+
 // Tunable shape lists (index 0 is the default). Only the large lengths, where
 // register pressure and occupancy trade against shared-memory passes, carry
 // alternatives; the autotuner measures them on the device.

@@ -191,6 +191,39 @@ int doe_random_phase(int nx, int ny, double seed, double* out);
 int doe_error_diffusion(doe_ctx* ctx, int batch, long long n, int levels, int snake, int wrap_first,
                         const double* phase, double* out);
 
+/* recordHologram -- src/interference.js:347-388: sum = object + reference,
+ * recorded = |sum|^2 / max, plate encoded as encode 0 'raw' (recorded), 1 'binary'
+ * (recorded > 0.5) or 2 'phase' (exp(i wrapPhase(arg sum)), quantised to `levels`
+ * when levels > 1). Host FP64 planes of n samples; sum_re / sum_im may be NULL. */
+int doe_hologram_record(doe_ctx* ctx, const double* obj_re, const double* obj_im, const double* ref_re,
+                        const double* ref_im, long long n, int encode, int levels, double* plate_re,
+                        double* plate_im, double* recorded, double* sum_re, double* sum_im);
+
+/* reconstructHologram -- src/interference.js:397-411: illumination = plate *
+ * reference, angular-spectrum propagated to +z (real image) and -z (virtual image)
+ * as one two-plane batch. The reference's default is band_limit = 0. illum_re /
+ * illum_im may be NULL. */
+int doe_hologram_reconstruct(doe_ctx* ctx, const double* plate_re, const double* plate_im,
+                             const double* ref_re, const double* ref_im, int nx, int ny, double dx, double dy,
+                             double lambda, double z, int band_limit, int evanescent, double soft_edge,
+                             double* real_re, double* real_im, double* virt_re, double* virt_im,
+                             double* illum_re, double* illum_im);
+
+/* modalIntensity -- src/interference.js:57-69: sum_m w_m |U_m|^2 / sum_m w_m over
+ * M modes [M][nx*ny] (weights NULL = all 1). With z != 0 every mode is first
+ * angular-spectrum propagated to z in one batch (the reference's tests propagate
+ * each mode with propagateAngularSpectrumInPlace, then call modalIntensity). */
+int doe_modal_intensity(doe_ctx* ctx, int modes, const double* re, const double* im, int nx, int ny,
+                        const double* weights, double dx, double dy, double lambda, double z, int band_limit,
+                        int evanescent, double soft_edge, double* out);
+
+/* partiallyCoherentModes -- src/interference.js:79-125: `modes` fields [modes][nx*ny]
+ * = Gaussian envelope exp(-(x^2+y^2)/waist^2) times exp(i phi), phi a uniform
+ * (-pi, pi] screen from one xorshift32 stream (src/doe.js:65-75) smoothed by a
+ * circular box blur of radius max(1, round(max(1, sigma/dx))) pixels. */
+int doe_partially_coherent_modes(doe_ctx* ctx, int nx, int ny, double dx, double dy, int modes, double sigma,
+                                 double waist, double seed, double* re, double* im);
+
 /* gerchbergSaxton / weightedGerchbergSaxton / fourierCgh on one design. */
 int doe_design(doe_ctx* ctx, const doe_design_desc* desc, doe_design_result* result);
 /* n designs sharing grid, pitch, algorithm and iterations, run as one batch. */

@@ -1192,3 +1192,131 @@ void orc_prepare_target(const double* irr, const double* illumination, long n, d
     for (long k = 0; k < n; k++) out[k] *= s;
   }
 }
+
+/* ------------------------------------------------------------------ */
+/* src/interference.js:57-69 modalIntensity over M modes [M][n]; w NULL = all 1. */
+void orc_modal_intensity(int M, const double* re, const double* im, long n, const double* w, double* out) {
+  double wsum = 0;
+  for (long k = 0; k < n; k++) out[k] = 0;
+  for (int m = 0; m < M; m++) {
+    double wm = w ? w[m] : 1;
+    wsum += wm;
+    const double* r = re + (long)m * n;
+    const double* q = im + (long)m * n;
+    for (long k = 0; k < n; k++) out[k] += wm * (r[k] * r[k] + q[k] * q[k]);
+  }
+  if (wsum > 0)
+    for (long k = 0; k < n; k++) out[k] /= wsum;
+}
+
+/* src/interference.js:347-388 recordHologram; encode 0 'raw', 1 'binary', 2 'phase'. */
+void orc_record_hologram(const double* obj_re, const double* obj_im, const double* ref_re, const double* ref_im,
+                         long n, int encode, int levels, double* plate_re, double* plate_im, double* recorded,
+                         double* sum_re, double* sum_im) {
+  for (long k = 0; k < n; k++) {
+    sum_re[k] = obj_re[k] + ref_re[k];
+    sum_im[k] = obj_im[k] + ref_im[k];
+  }
+  for (long k = 0; k < n; k++) recorded[k] = sum_re[k] * sum_re[k] + sum_im[k] * sum_im[k];
+  double norm = 0;
+  for (long k = 0; k < n; k++)
+    if (recorded[k] > norm) norm = recorded[k];
+  if (norm > 0)
+    for (long k = 0; k < n; k++) recorded[k] /= norm;
+  for (long k = 0; k < n; k++) {
+    plate_re[k] = 0;
+    plate_im[k] = 0;
+  }
+  if (encode == 0) {
+    for (long k = 0; k < n; k++) plate_re[k] = recorded[k];
+  } else if (encode == 1) {
+    for (long k = 0; k < n; k++) plate_re[k] = recorded[k] > 0.5 ? 1 : 0;
+  } else {
+    for (long k = 0; k < n; k++) {
+      double ph = wrap1(atan2(sum_im[k], sum_re[k]));
+      plate_re[k] = cos(ph);
+      plate_im[k] = sin(ph);
+    }
+    if (levels > 1) {
+      double step = (2 * M_PI) / levels;
+      for (long k = 0; k < n; k++) {
+        double ph = js_round(atan2(plate_im[k], plate_re[k]) / step) * step;
+        plate_re[k] = cos(ph);
+        plate_im[k] = sin(ph);
+      }
+    }
+  }
+}
+
+/* src/interference.js:397-411 reconstructHologram: illumination = plate * reference,
+ * then angular-spectrum propagation of two copies to +z (real) and -z (virtual). */
+void orc_reconstruct_hologram(const double* plate_re, const double* plate_im, const double* ref_re,
+                              const double* ref_im, int nx, int ny, double dx, double dy, double lambda, double z,
+                              int band_limit, int evanescent, double soft_edge, double* real_re, double* real_im,
+                              double* virt_re, double* virt_im, double* illum_re, double* illum_im) {
+  long n = (long)nx * ny;
+  for (long k = 0; k < n; k++) {
+    illum_re[k] = plate_re[k] * ref_re[k] - plate_im[k] * ref_im[k];
+    illum_im[k] = plate_re[k] * ref_im[k] + plate_im[k] * ref_re[k];
+  }
+  memcpy(real_re, illum_re, sizeof(double) * n);
+  memcpy(real_im, illum_im, sizeof(double) * n);
+  memcpy(virt_re, illum_re, sizeof(double) * n);
+  memcpy(virt_im, illum_im, sizeof(double) * n);
+  orc_asm_inplace(real_re, real_im, nx, ny, dx, dy, lambda, z, band_limit, evanescent, soft_edge);
+  orc_asm_inplace(virt_re, virt_im, nx, ny, dx, dy, lambda, -z, band_limit, evanescent, soft_edge);
+}
+
+/* src/interference.js:104-125 smoothInPlace: separable circular box blur of
+ * radius r by running sums (rows into tmp, then columns back into arr). */
+static void box_blur_circular(double* arr, int nx, int ny, int r) {
+  long n = (long)nx * ny;
+  double* tmp = (double*)malloc(sizeof(double) * n);
+  double norm = 1.0 / (2 * r + 1);
+  for (int j = 0; j < ny; j++) {
+    double acc = 0;
+    for (int i = -r; i <= r; i++) acc += arr[((i % nx) + nx) % nx + (long)j * nx];
+    for (int i = 0; i < nx; i++) {
+      tmp[i + (long)j * nx] = acc * norm;
+      acc -= arr[(((i - r) % nx) + nx) % nx + (long)j * nx];
+      acc += arr[(((i + r + 1) % nx) + nx) % nx + (long)j * nx];
+    }
+  }
+  for (int i = 0; i < nx; i++) {
+    double acc = 0;
+    for (int j = -r; j <= r; j++) acc += tmp[i + (long)(((j % ny) + ny) % ny) * nx];
+    for (int j = 0; j < ny; j++) {
+      arr[i + (long)j * nx] = acc * norm;
+      acc -= tmp[i + (long)((((j - r) % ny) + ny) % ny) * nx];
+      acc += tmp[i + (long)((((j + r + 1) % ny) + ny) % ny) * nx];
+    }
+  }
+  free(tmp);
+}
+
+/* src/interference.js:79-101 partiallyCoherentModes: M modes [M][n] from one
+ * xorshift32 stream (src/doe.js:65-75), each a Gaussian envelope of waist
+ * `waist` times a box-smoothed uniform phase screen. */
+void orc_partially_coherent_modes(int nx, int ny, double dx, double dy, int modes, double sigma, double waist,
+                                  double seed, double* re, double* im) {
+  long n = (long)nx * ny;
+  uint32_t st = orc_rng_seed(seed);
+  double sigma_pix = fmax(1, sigma / dx);
+  int r = (int)fmax(1, js_round(sigma_pix));
+  double* ph = (double*)malloc(sizeof(double) * n);
+  for (int m = 0; m < modes; m++) {
+    for (long k = 0; k < n; k++) ph[k] = (orc_rng_next(&st) * 2 - 1) * M_PI;
+    box_blur_circular(ph, nx, ny, r);
+    for (int j = 0; j < ny; j++) {
+      double y = (j - ny / 2.0) * dy;
+      for (int i = 0; i < nx; i++) {
+        double x = (i - nx / 2.0) * dx;
+        long k = i + (long)j * nx;
+        double a = exp(-(x * x + y * y) / (waist * waist));
+        re[(long)m * n + k] = a * cos(ph[k]);
+        im[(long)m * n + k] = a * sin(ph[k]);
+      }
+    }
+  }
+  free(ph);
+}

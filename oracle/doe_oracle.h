@@ -138,6 +138,21 @@ void orc_screen_metrics_full(const double* field_re, const double* field_im, int
 /* src/doe.js:817-829 target amplitude and power match. */
 void orc_prepare_target(const double* irr, const double* illumination, long n, double* out);
 
+/* src/interference.js:57-69 modalIntensity of M modes [M][n] (w NULL = all 1). */
+void orc_modal_intensity(int M, const double* re, const double* im, long n, const double* w, double* out);
+/* src/interference.js:347-388 recordHologram (encode 0 raw, 1 binary, 2 phase). */
+void orc_record_hologram(const double* obj_re, const double* obj_im, const double* ref_re, const double* ref_im,
+                         long n, int encode, int levels, double* plate_re, double* plate_im, double* recorded,
+                         double* sum_re, double* sum_im);
+/* src/interference.js:397-411 reconstructHologram (real image at +z, virtual at -z). */
+void orc_reconstruct_hologram(const double* plate_re, const double* plate_im, const double* ref_re,
+                              const double* ref_im, int nx, int ny, double dx, double dy, double lambda, double z,
+                              int band_limit, int evanescent, double soft_edge, double* real_re, double* real_im,
+                              double* virt_re, double* virt_im, double* illum_re, double* illum_im);
+/* src/interference.js:79-125 partiallyCoherentModes, modes [M][n]. */
+void orc_partially_coherent_modes(int nx, int ny, double dx, double dy, int modes, double sigma, double waist,
+                                  double seed, double* re, double* im);
+
 #ifdef __cplusplus
 }
 #endif

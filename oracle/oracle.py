@@ -91,6 +91,10 @@ def lib():
         L.orc_error_diffusion.argtypes = [_dp, C.c_long, i, i, i, _dp]
         L.orc_screen_metrics_full.argtypes = [_dp, _dp, i, i, d, d, _dp, _dp, _dp, _dp, d, d, i, i, _dp]
         L.orc_prepare_target.argtypes = [_dp, _dp, C.c_long, _dp]
+        L.orc_modal_intensity.argtypes = [i, _dp, _dp, C.c_long, _dp, _dp]
+        L.orc_record_hologram.argtypes = [_dp, _dp, _dp, _dp, C.c_long, i, i, _dp, _dp, _dp, _dp, _dp]
+        L.orc_reconstruct_hologram.argtypes = [_dp, _dp, _dp, _dp, i, i, d, d, d, d, i, i, d] + [_dp] * 6
+        L.orc_partially_coherent_modes.argtypes = [i, i, d, d, i, d, d, d, _dp, _dp]
         _lib = L
     return _lib
 
@@ -343,3 +347,46 @@ def multiplane(illumination, zs, target_amps, rois, weights, *, nx, ny, dx, dy=N
         raise RuntimeError(f"oracle multiplane failed ({rc})")
     return dict(phase=phase, error=err[:iterations], efficiency=eff[:iterations],
                 perPlaneError=ppe.reshape(P, -1)[:, :iterations])
+
+
+def modal_intensity(re, im, n, weights=None):
+    """modalIntensity (src/interference.js:57-69) of modes [M][n]."""
+    r, i = _f64(re), _f64(im)
+    M = r.size // n
+    w = None if weights is None else _f64(weights)
+    out = np.empty(n)
+    lib().orc_modal_intensity(M, _p(r), _p(i), n, _p(w), _p(out))
+    return out
+
+
+HOLOGRAM_ENCODINGS = {"raw": 0, "binary": 1, "phase": 2}
+
+
+def record_hologram(obj_re, obj_im, ref_re, ref_im, encode="raw", levels=0):
+    """recordHologram (src/interference.js:347-388) -> dict of plate/recorded/sum planes."""
+    a = [_f64(v) for v in (obj_re, obj_im, ref_re, ref_im)]
+    n = a[0].size
+    out = {k: np.empty(n) for k in ("plate_re", "plate_im", "recorded", "sum_re", "sum_im")}
+    lib().orc_record_hologram(*[_p(v) for v in a], n, HOLOGRAM_ENCODINGS[encode], int(levels),
+                              *[_p(out[k]) for k in ("plate_re", "plate_im", "recorded", "sum_re", "sum_im")])
+    return out
+
+
+def reconstruct_hologram(plate_re, plate_im, ref_re, ref_im, nx, ny, dx, dy, lam, z, band_limit=False,
+                         evanescent=True, soft_edge=0.02):
+    """reconstructHologram (src/interference.js:397-411), bandLimit false by default as there."""
+    a = [_f64(v) for v in (plate_re, plate_im, ref_re, ref_im)]
+    n = nx * ny
+    keys = ("real_re", "real_im", "virt_re", "virt_im", "illum_re", "illum_im")
+    out = {k: np.empty(n) for k in keys}
+    lib().orc_reconstruct_hologram(*[_p(v) for v in a], nx, ny, dx, dy, lam, z, int(band_limit),
+                                   int(evanescent), soft_edge, *[_p(out[k]) for k in keys])
+    return out
+
+
+def partially_coherent_modes(nx, ny, dx, dy, modes=8, sigma=40e-6, waist=1e-3, seed=7):
+    """partiallyCoherentModes (src/interference.js:79-125) -> (re, im) of shape [modes, nx*ny]."""
+    n = nx * ny
+    re, im = np.empty(modes * n), np.empty(modes * n)
+    lib().orc_partially_coherent_modes(nx, ny, dx, dy, modes, sigma, waist, float(seed), _p(re), _p(im))
+    return re.reshape(modes, n), im.reshape(modes, n)
