@@ -209,7 +209,10 @@ inline int ilog2i(int n) {
 
 template <class S, class Op>
 inline int launch_row(doe_ctx* c, const Op& op, int nplanes, int nlines, cudaStream_t stream = nullptr) {
-  auto kern = row_kernel<S, Op>;
+  auto kern = [] {
+    if constexpr (S::MINB > 1) return row_kernel_capped<S, Op>;
+    else return row_kernel<S, Op>;
+  }();
   static unsigned long long attr_set = 0;  // one bit per device
   if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
     DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
@@ -228,7 +231,10 @@ inline int launch_row(doe_ctx* c, const Op& op, int nplanes, int nlines, cudaStr
 
 template <class S, class Op>
 inline int launch_col(doe_ctx* c, const Op& op, int nplanes, int ncols, cudaStream_t stream = nullptr) {
-  auto kern = col_kernel<S, Op>;
+  auto kern = [] {
+    if constexpr (S::MINB > 1) return col_kernel_capped<S, Op>;
+    else return col_kernel<S, Op>;
+  }();
   static unsigned long long attr_set = 0;  // one bit per device
   if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
     DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));

@@ -28,21 +28,23 @@ struct NoAcc {};
 // CTA shapes. A row shape processes V vectors of a plane per CTA (one vector =
 // one row), a column shape C adjacent columns (element-major tile in shared
 // memory so a half-warp always touches one element row: conflict-free).
-template <class P, int V_>
+template <class P, int V_, int MINB_ = 1>
 struct RowShape {
   using Plan = P;
   static constexpr int N = P::N;
   static constexpr int V = V_;
+  static constexpr int MINB = MINB_;  // CTAs per SM the register budget is sized for
   static constexpr int T = P::T;
   static constexpr int THREADS = V * T;
   static constexpr int SMEM = P::NP > 1 ? V * padded_len<P::N>() * (int)sizeof(float2) : 0;
 };
 
-template <class P, int C_>
+template <class P, int C_, int MINB_ = 1>
 struct ColShape {
   using Plan = P;
   static constexpr int N = P::N;
   static constexpr int C = C_;
+  static constexpr int MINB = MINB_;  // CTAs per SM the register budget is sized for
   static constexpr int T = P::T;
   static constexpr int THREADS = C * T;
   static constexpr int SMEM = P::NP > 1 ? (P::N * C + (P::N * C) / 32 + 1) * (int)sizeof(float2) : 0;
@@ -63,10 +65,20 @@ struct DefCol {
   using type = ColShape<P, C>;
 };
 
-// 2048-point columns: radix 32-2-32 with 4 columns per CTA (256 threads, 128
-// registers, no spills) beats the default 16-8-16 plan with 512-thread CTAs in
-// the design loops' two-transform column passes on B200; rows keep the default
-// (their fused operators spill at RMAX 32).
+// 2048-point rows: the default plan, with registers capped for three 256-thread
+// CTAs per SM (the design loops' fused row operators otherwise take ~100-128
+// registers, two CTAs per SM, and stall on memory latency).
+template <>
+struct DefRow<2048> {
+  using type = RowShape<typename DefaultPlan<2048>::type, 2, 3>;
+};
+
+// 2048-point columns: radix 32-2-32 with 4 columns per CTA (256 threads; the
+// design loops' two-transform column operators use ~254 registers, one CTA per
+// SM, no spills) beats the default 16-8-16 plan with 512-thread CTAs in those
+// column passes on B200 (~12 % less time per pass; capping the 16-8-16 plan at
+// three 256-thread CTAs per SM spills and is ~45 % slower); rows keep the default
+// plan (their fused operators spill at RMAX 32).
 template <>
 struct DefCol<2048> {
   using type = ColShape<FftPlan<2048, 3, 32, 2, 32>, 4>;
@@ -146,7 +158,7 @@ __device__ __forceinline__ bool op_skip(const Op& op, int plane) {
 
 // Row pass. Grid: nplanes * ceil(nlines / V) CTAs; rows beyond nlines idle.
 template <class S, class Op>
-__global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __restrict__ tw, int nlines) {
+__device__ __forceinline__ void row_pass(const Op& op, const float2* __restrict__ tw, int nlines) {
   using P = typename S::Plan;
   constexpr int T = P::T;
   constexpr int V = S::V;
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __
 
 // Column pass. Grid: (ceil(ncols / C), nplanes); columns beyond ncols idle.
 template <class S, class Op>
-__global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __restrict__ tw, int ncols) {
+__device__ __forceinline__ void col_pass(const Op& op, const float2* __restrict__ tw, int ncols) {
   using P = typename S::Plan;
   constexpr int C = S::C;
   constexpr int RMAX = P::RMAX;
@@ -233,6 +245,28 @@ __global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __
     for (int q = 0; q < RMAX; ++q) op.store(st, out_elem<P>(t, q), v[q], acc);
   }
   op.finish(plane, blockIdx.x, gridDim.x, acc);
+}
+
+// The kernels. Shapes with MINB > 1 get the register cap of MINB resident CTAs
+// per SM; the others leave the register budget to the compiler (an explicit
+// minimum of one CTA per SM lets it use all 255 registers, which costs occupancy).
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS) row_kernel(Op op, const float2* __restrict__ tw, int nlines) {
+  row_pass<S, Op>(op, tw, nlines);
+}
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS, S::MINB) row_kernel_capped(Op op, const float2* __restrict__ tw,
+                                                                         int nlines) {
+  row_pass<S, Op>(op, tw, nlines);
+}
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS) col_kernel(Op op, const float2* __restrict__ tw, int ncols) {
+  col_pass<S, Op>(op, tw, ncols);
+}
+template <class S, class Op>
+__global__ void __launch_bounds__(S::THREADS, S::MINB) col_kernel_capped(Op op, const float2* __restrict__ tw,
+                                                                         int ncols) {
+  col_pass<S, Op>(op, tw, ncols);
 }
 
 // ---------------------------------------------------------------- FP64 reductions

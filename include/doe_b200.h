@@ -72,11 +72,12 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
 
 /* Tuning knobs (engine-only): "sweep_group" = planes per focus-sweep launch pair
  * (0 = sized from the L2 cache); "sweep_fused" = 1 to read and multiply per
- * element in the sweep column pass (0: all reads first); "fft_row", "fft_col",
+ * element in the sweep column pass (0: all reads first); "sweep_graph" = 0 to
+ * disable CUDA-graph replay of repeated device sweeps; "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
-/* Current value of "sweep_group" or "sweep_fused". */
+/* Current value of "sweep_group", "sweep_fused" or "sweep_graph". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for
