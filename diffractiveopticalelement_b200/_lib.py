@@ -114,6 +114,7 @@ def _declare(L):
         "doe_design": (i, [ctxp, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_random_phase": (i, [i, i, d, _dp]),
         "doe_simulate": (i, [ctxp, _dp, _dp, i, i, d, d, d, d, i, i, i, _dp, _dp, _dp]),
+        "doe_simulate_sweep": (i, [ctxp, _dp, _dp, i, i, d, d, d, _dp, i, i, i, i, _dp, _dp, _dp]),
         "doe_screen_metrics": (i, [ctxp, _dp, _dp, i, i, d, d, _dp, _dp, _dp, d, d, _dp]),
         "doe_screen_metrics_dev": (i, [ctxp, i, i, i, _vp, _vp, C.c_longlong, _vp, _vp, C.c_longlong, d, d, d, d,
                                        _vp]),

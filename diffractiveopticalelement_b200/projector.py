@@ -245,30 +245,56 @@ class ProjectorSystem:
             m["spotUniformity"] = None
         return m
 
+    def simulateMany(self, zs, opts=None):
+        """simulate (src/projector.js:475-498) at every distance of `zs` in one engine
+        call (doe_simulate_sweep): the element's forward transform is shared."""
+        opts = opts or {}
+        if self.result is None:
+            raise RuntimeError("ProjectorSystem.simulate: call design() first")
+        zs = np.ascontiguousarray([self.z if z is None else z for z in zs], dtype=np.float64)
+        mode = opts.get("mode") or self.cfg["mode"]
+        phase = opts.get("phase")
+        phase = self.result["phase"] if phase is None else phase
+        far = mode == "far-field"
+        n = self.nx * self.ny
+        re = np.empty(zs.size * n)
+        im = np.empty(zs.size * n)
+        d = np.zeros(2 * zs.size)
+        c = self.ctx or _lib.context()
+        c.check(c.lib.doe_simulate_sweep(c.h, _lib.dp(_lib.f64(self.result["illumination"])),
+                                         _lib.dp(_lib.f64(phase)), self.nx, self.ny, self.dx, self.dy, self.lam,
+                                         _lib.dp(zs), int(zs.size), int(bool(opts.get("bandLimit", False))),
+                                         int(far), int(opts.get("pad", 1)), _lib.dp(re), _lib.dp(im), _lib.dp(d)))
+        out = []
+        for k in range(zs.size):
+            f = ComplexField(self.nx, self.ny, float(d[2 * k]), float(d[2 * k + 1]))
+            f.re = re[k * n:(k + 1) * n]
+            f.im = im[k * n:(k + 1) * n]
+            out.append(f)
+        return out
+
     def defocusCurve(self, opts=None):
-        """src/projector.js:622-642."""
+        """src/projector.js:622-642; the planes come from one simulateMany call."""
         opts = opts or {}
         points, span = opts.get("points", 21), opts.get("span", 0.6)
         z0, z1 = self.z * (1 - span), self.z * (1 + span)
+        zs = [z0 + ((z1 - z0) * i) / (points - 1) for i in range(points)]
+        fields = self.simulateMany(zs, {"pad": opts.get("pad", 2), "mode": opts.get("mode")})
         out = []
-        for i in range(points):
-            z = z0 + ((z1 - z0) * i) / (points - 1)
-            m = self.screenMetrics(self.simulate({"z": z, "pad": opts.get("pad", 2), "mode": opts.get("mode")}))
+        for z, field in zip(zs, fields):
+            m = self.screenMetrics(field)
             out.append({"z": z, "zMm": z * 1e3, "fidelity": m["fidelity"], "correlation": m["correlation"],
                         "ssim": m["ssim"], "rmse": m["rmse"], "efficiency": m["efficiency"],
                         "uniformity": m["uniformity"]})
         return out
 
     def focusStack(self, opts=None):
-        """src/projector.js:645-653."""
+        """src/projector.js:645-653; the planes come from one simulateMany call."""
         opts = opts or {}
         points, span = opts.get("points", 9), opts.get("span", 0.5)
-        planes = []
-        for i in range(points):
-            z = self.z * (1 - span) + (self.z * 2 * span * i) / (points - 1)
-            f = self.simulate({"z": z, "pad": opts.get("pad", 2), "mode": opts.get("mode")})
-            planes.append({"z": z, "intensity": f.intensity()})
-        return planes
+        zs = [self.z * (1 - span) + (self.z * 2 * span * i) / (points - 1) for i in range(points)]
+        fields = self.simulateMany(zs, {"pad": opts.get("pad", 2), "mode": opts.get("mode")})
+        return [{"z": z, "intensity": f.intensity()} for z, f in zip(zs, fields)]
 
     def designMultiPlane(self, planeSpecs, opts=None):
         """src/projector.js:675-712."""

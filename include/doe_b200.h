@@ -325,6 +325,16 @@ int doe_simulate(doe_ctx* ctx, const double* illumination, const double* phase, 
                  double dx, double dy, double lambda, double z, int band_limit, int far_field,
                  int pad, double* out_re, double* out_im, double* out_d);
 
+/* ProjectorSystem.simulate at nz distances z[] (defocusCurve / focusStack,
+ * src/projector.js:622-653, call simulate once per distance): the element's
+ * forward transform is computed once and shared by every distance. out_re /
+ * out_im are [nz][nx*ny]; out_d (may be NULL) receives nz (dx, dy) pairs, the
+ * screen pitch of each plane (lens throws give lambda*z/(n*dx)). Same planes as
+ * nz calls of doe_simulate. */
+int doe_simulate_sweep(doe_ctx* ctx, const double* illumination, const double* phase, int nx, int ny,
+                       double dx, double dy, double lambda, const double* z, int nz, int band_limit,
+                       int far_field, int pad, double* out_re, double* out_im, double* out_d);
+
 /* ProjectorSystem.screenMetrics, radiometric subset -- src/projector.js:554-595
  * with src/metrics.js:10-18, :73-84: out = {rmse, efficiency, fluxFraction,
  * powerInSignal, powerAtScreen, powerIncident}. roi may be NULL. */

@@ -133,3 +133,44 @@ def test_multiplane_projector_runs(engine):
                               {"iterations": 10})
     assert r["mode"] == "multi-plane" and len(r["error"]) == 10 and len(r["perPlaneError"]) == 2
     assert r["error"][-1] < r["error"][0]
+
+
+@pytest.mark.parametrize("mode,pad,bl", [("image-plane", 2, False), ("image-plane", 1, True), ("far-field", 1, False)])
+def test_simulate_many_equals_per_distance_simulate(engine, oracle, mode, pad, bl):
+    """One engine call for many distances (shared forward transform) gives the
+    planes of one simulate call per distance, z = 0 included in the near field."""
+    n, dx = 128, 8e-6
+    sys_ = engine.ProjectorSystem({**BASE, "mode": mode})
+    sys_.result = {"illumination": oracle.disc_mask(n, n, dx, dx, 0.45 * n * dx, 2 * dx),
+                   "phase": oracle.random_phase(n, n, 9)}
+    zs = [0.012, 0.03, 0.047, 0.0211] + ([] if mode == "far-field" else [0.0, -0.02])
+    many = sys_.simulateMany(zs, {"pad": pad, "bandLimit": bl})
+    for z, f in zip(zs, many):
+        one = sys_.simulate({"z": z, "pad": pad, "bandLimit": bl})
+        assert (f.dx, f.dy) == (one.dx, one.dy)
+        if mode == "far-field" or z == 0.0:
+            assert np.array_equal(f.re, one.re) and np.array_equal(f.im, one.im)
+        else:
+            assert rel_l2(f.re + 1j * f.im, one.re + 1j * one.im) < 1e-6
+
+
+@pytest.mark.parametrize("mode", ["image-plane", "far-field"])
+def test_defocus_curve_and_focus_stack(engine, mode):
+    """defocusCurve (src/projector.js:622-642) and focusStack (:645-653): distances,
+    per-plane metrics equal to screenMetrics(simulate(z)), best focus at the design
+    distance for the image-plane design."""
+    sys_ = engine.ProjectorSystem({**BASE, "n": 64, "mode": mode, "target": {"kind": "disc"}})
+    sys_.design()
+    curve = sys_.defocusCurve({"points": 7, "span": 0.6})
+    assert len(curve) == 7
+    assert curve[3]["z"] == pytest.approx(sys_.z)
+    for p in (curve[0], curve[3], curve[6]):
+        m = sys_.screenMetrics(sys_.simulate({"z": p["z"], "pad": 2}))
+        for k in ("rmse", "efficiency", "correlation", "ssim", "uniformity"):
+            assert p[k] == pytest.approx(m[k], rel=1e-4, abs=1e-9)
+    if mode == "image-plane":
+        assert min(range(7), key=lambda i: curve[i]["rmse"]) == 3
+    stack = sys_.focusStack({"points": 5})
+    assert [round(s["z"] / sys_.z, 6) for s in stack] == [0.5, 0.75, 1.0, 1.25, 1.5]
+    mid = sys_.simulate({"z": stack[2]["z"], "pad": 2}).intensity()
+    assert rel_l2(stack[2]["intensity"], mid) < 1e-6
