@@ -66,6 +66,12 @@ struct DesignBufs {
 
 __device__ __forceinline__ int rotn(int i, int n) { return (i + (n >> 1)) & (n - 1); }
 
+// Pull the line holding *p into L1. The design passes read their side planes
+// (targets, masks, weights, illumination, transfer tables) only after a transform
+// stage; touching them in the load step, before that stage, turns those later
+// reads from DRAM-latency misses into L1 hits.
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // Designs that met the screen goal drop out of every later pass (whole CTAs
 // return before any barrier: the plane index is uniform per CTA).
 __device__ __forceinline__ bool design_stopped(const DesignState* st, int p) { return st && st[p].stop >= 0; }
@@ -105,6 +111,7 @@ struct ColAsmTab : NoReduce {
   __device__ __forceinline__ State init(int p, int x) const {
     return {w + p * (long)nx * ny + x, htab + p * htab_stride + x};
   }
+  __device__ __forceinline__ void prefetch(const State& s, int y) const { prefetch_l1(&s.h[(long)y * nx]); }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.w[(long)y * nx]; }
   __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc&) const {
     const float2 h = __ldg(&s.h[(long)y * nx]);
@@ -138,6 +145,12 @@ struct ColFourier {
     const long ot = p * b.tgt_stride + rotn(x, b.nx);
     return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, WGS ? b.wraw + o : nullptr, b.amp + o,
             b.W + p * b.pe() + x, WGS ? (float)b.st[p].norm : 1.f};
+  }
+  __device__ __forceinline__ void prefetch(const State& s, int y) const {
+    const long j = (long)rotn(y, b.ny) * b.nx;
+    prefetch_l1(&s.t[j]);
+    if (s.m) prefetch_l1(&s.m[j]);
+    if constexpr (WGS) prefetch_l1(&s.w[j]);
   }
   __device__ __forceinline__ float2 load(const State& s, int y) const { return s.W[(long)y * b.nx]; }
   __device__ __forceinline__ void mid(const State& s, int y, float2& v, Acc& acc) const {
@@ -263,6 +276,13 @@ struct RowDoeUpdate : NoReduce {
     return {b.illum + o, b.phase + o, SNAP ? b.best_phase + o : nullptr, SNAP ? b.amp + o : nullptr,
             SNAP ? b.best_amp + o : nullptr, b.W + p * pe + (long)y * b.nx, snap};
   }
+  __device__ __forceinline__ void prefetch(const State& s, int x) const {
+    const int xi = ROT ? rotn(x, b.nx) : x;
+    prefetch_l1(&s.A[xi]);
+    if constexpr (SNAP) {
+      if (s.snap) prefetch_l1(&s.amp[xi]);
+    }
+  }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
   __device__ __forceinline__ float2 doe(const State& s, int x, float2 v) const {
     const int xi = ROT ? rotn(x, b.nx) : x;
@@ -316,6 +336,10 @@ struct RowGsTarget {
     const long ot = p * b.tgt_stride + (long)y * b.nx;
     const float fb = (!MP && it >= b.escape) ? b.feedback : 0.f;
     return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.amp + o, b.W + o, fb};
+  }
+  __device__ __forceinline__ void prefetch(const State& s, int x) const {
+    prefetch_l1(&s.t[x]);
+    if (s.m) prefetch_l1(&s.m[x]);
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
   __device__ __forceinline__ float measure(const State& s, int x, float2 u, Acc& acc) const {
@@ -409,6 +433,14 @@ struct RowWgsTarget {
     const long ot = p * b.tgt_stride + (long)y * b.nx;
     return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o,
             (GOAL && b.screen_irr) ? b.screen_irr + o : nullptr, (float)b.st[p].norm};
+  }
+  __device__ __forceinline__ void prefetch(const State& s, int x) const {
+    prefetch_l1(&s.t[x]);
+    if (s.m) prefetch_l1(&s.m[x]);
+    if constexpr (!INITIAL) prefetch_l1(&s.w[x]);
+    if constexpr (GOAL) {
+      if (s.T) prefetch_l1(&s.T[x]);
+    }
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.W[x]; }
   __device__ __forceinline__ void mid(const State&, int, float2&, Acc&) const {}
@@ -518,8 +550,16 @@ struct RowWgsConstrain : NoReduce {
     return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, b.phase + o,
             b.best_phase + o, b.best_amp + o, (float)b.st[p].norm, snap};
   }
+  // every field read and side-plane prefetch of the thread first, then the
+  // constraint (whose snapshot stores would otherwise keep later reads waiting)
   __device__ __forceinline__ float2 load(const State& s, int x) const {
-    const float2 u = __ldg(&s.U[x]);
+    prefetch_l1(&s.t[x]);
+    prefetch_l1(&s.w[x]);
+    if (s.m) prefetch_l1(&s.m[x]);
+    if (s.snap) prefetch_l1(&s.ph[x]);
+    return __ldg(&s.U[x]);
+  }
+  __device__ __forceinline__ float2 finish_load(const State& s, int x, float2 u) const {
     const float m = s.m ? __ldg(&s.m[x]) : 1.f;
     const float t = __ldg(&s.t[x]);
     const float w = __ldg(&s.w[x]);
@@ -560,6 +600,10 @@ struct RowLossField {
     const long o = p * b.pe() + (long)y * b.nx;
     const long ot = p * b.tgt_stride + (long)y * b.nx;
     return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.W + o};
+  }
+  __device__ __forceinline__ void prefetch(const State& s, int x) const {
+    prefetch_l1(&s.t[x]);
+    if (s.m) prefetch_l1(&s.m[x]);
   }
   __device__ __forceinline__ float2 load(const State& s, int x) const { return s.w[x]; }
   __device__ __forceinline__ void mid(const State& s, int x, float2& v, Acc& acc) const {

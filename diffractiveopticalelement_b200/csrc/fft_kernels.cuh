@@ -84,6 +84,12 @@ struct DefCol<2048> {
   using type = ColShape<FftPlan<2048, 3, 32, 2, 32>, 4>;
 };
 
+// 256-point columns: registers capped for two CTAs of 16 columns per SM.
+template <>
+struct DefCol<256> {
+  using type = ColShape<typename DefaultPlan<256>::type, 16, 2>;
+};
+
 // Tunable shape lists (index 0 is the default). Only the large lengths, where
 // register pressure and occupancy trade against shared-memory passes, carry
 // alternatives; the autotuner measures them on the device.
@@ -147,6 +153,17 @@ template <class Op>
 struct HasFinishLoad<Op, std::void_t<decltype(std::declval<const Op&>().finish_load(
                              std::declval<const typename Op::State&>(), 0, float2{}))>> : std::true_type {};
 
+// Operators may expose `prefetch(state, e)`: it touches the lines of side planes
+// that a later stage of the pass reads for element e, and runs just before the
+// element's load. Column passes use it up to 1024 points only: the 2048-point
+// design column operators need ~250 registers without it and the extra addresses
+// cost them more than the hidden latency saves.
+template <class Op, class = void>
+struct HasPrefetch : std::false_type {};
+template <class Op>
+struct HasPrefetch<Op, std::void_t<decltype(std::declval<const Op&>().prefetch(
+                           std::declval<const typename Op::State&>(), 0))>> : std::true_type {};
+
 template <class Op>
 __device__ __forceinline__ bool op_skip(const Op& op, int plane) {
   if constexpr (HasSkip<Op>::value) {
@@ -178,7 +195,10 @@ __device__ __forceinline__ void row_pass(const Op& op, const float2* __restrict_
   float2 v[RMAX];
   if (active) {
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+    for (int q = 0; q < RMAX; ++q) {
+      if constexpr (HasPrefetch<Op>::value) op.prefetch(st, in_elem<P>(t, q));
+      v[q] = op.load(st, in_elem<P>(t, q));
+    }
     if constexpr (HasFinishLoad<Op>::value) {
 #pragma unroll
       for (int q = 0; q < RMAX; ++q) v[q] = op.finish_load(st, in_elem<P>(t, q), v[q]);
@@ -222,7 +242,10 @@ __device__ __forceinline__ void col_pass(const Op& op, const float2* __restrict_
   float2 v[RMAX];
   if (active) {
 #pragma unroll
-    for (int q = 0; q < RMAX; ++q) v[q] = op.load(st, in_elem<P>(t, q));
+    for (int q = 0; q < RMAX; ++q) {
+      if constexpr (HasPrefetch<Op>::value && S::N <= 1024) op.prefetch(st, in_elem<P>(t, q));
+      v[q] = op.load(st, in_elem<P>(t, q));
+    }
     if constexpr (HasFinishLoad<Op>::value) {
 #pragma unroll
       for (int q = 0; q < RMAX; ++q) v[q] = op.finish_load(st, in_elem<P>(t, q), v[q]);
