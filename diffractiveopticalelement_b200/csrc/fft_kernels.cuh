@@ -109,8 +109,9 @@ struct RowVariants<1024> {
 template <>
 struct ColVariants<1024> {
   using list = std::tuple<ColShape<FftPlan<1024, 2, 32, 32>, 8>, ColShape<FftPlan<1024, 3, 16, 4, 16>, 4>,
-                          ColShape<FftPlan<1024, 3, 16, 4, 16>, 8>, ColShape<FftPlan<1024, 2, 32, 32>, 4>>;
-};
+                          ColShape<FftPlan<1024, 3, 16, 4, 16>, 8>, ColShape<FftPlan<1024, 2, 32, 32>, 4>,
+                          ColShape<FftPlan<1024, 3, 16, 4, 16>, 4, 4>, ColShape<FftPlan<1024, 3, 16, 4, 16>, 2, 6>>;
+};  // the last two cap registers for 4 x 256 and 6 x 128 threads per SM (the sweep column pass picks the first)
 template <>
 struct RowVariants<2048> {
   using list = std::tuple<RowShape<FftPlan<2048, 3, 16, 8, 16>, 2>, RowShape<FftPlan<2048, 3, 32, 2, 32>, 4>,
