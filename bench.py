@@ -790,6 +790,10 @@ def main():
     ap.add_argument("--no-wgs", action="store_true", help="skip the WGS block of the default line")
     ap.add_argument("--surrogate-steps", type=int, default=1500,
                     help="training steps of the warm-start surrogate in the wgs256 workload (0: skip the warm arm)")
+    ap.add_argument("--pin-tuning", default=None,
+                    help="profiling runs: skip the autotuner (its timings are distorted under a profiler) and set "
+                         "these variants instead, e.g. fft_row=3,fft_col=0,sweep_row=3,sweep_col=4,sweep_fused=1,"
+                         "sweep_group=64 (the choices the tuner makes on B200)")
     ap.add_argument("--fields", type=int, default=NFIELDS,
                     help="fields per step (profiling runs use fewer; the benchmark uses 64)")
     args = ap.parse_args()
@@ -839,7 +843,21 @@ def main():
     L.doe_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.POINTER(C.c_int)]
     chosen = (C.c_int * 5)()
-    ctx.check(L.doe_autotune(ctx.h, NX, NY, DX, DX, 532e-9, 0.03, chosen))
+    if args.pin_tuning:
+        lg = int(math.log2(NX))
+        slots = {"fft_row": 0, "fft_col": 1, "sweep_row": 2, "sweep_col": 3}
+        for item in args.pin_tuning.split(","):
+            key, val = item.split("=")
+            val = int(val)
+            if key in slots:
+                ctx.check(L.doe_ctx_set_tuning(ctx.h, key.encode(), (lg << 8) | val))
+                chosen[slots[key]] = val
+            else:
+                ctx.check(L.doe_ctx_set_tuning(ctx.h, key.encode(), val))
+                if key == "sweep_group":
+                    chosen[4] = val
+    else:
+        ctx.check(L.doe_autotune(ctx.h, NX, NY, DX, DX, 532e-9, 0.03, chosen))
     fused = C.c_longlong(0)
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_fused", C.byref(fused)))
     graph = C.c_longlong(0)
@@ -900,7 +918,7 @@ def main():
         achieved = bytes_per_launch / avg_s / 1e9
         # DRAM bytes of one full-size sweep column launch (64 planes), ncu capture in
         # profiles/asm_sweep_col_1024.md; other kernels have no full-size capture
-        traffic = 494.03e6 * planes_per_launch / 64 if name == "asm_sweep_col" else None
+        traffic = 517.09e6 * planes_per_launch / 64 if name == "asm_sweep_col" else None
         roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch",
