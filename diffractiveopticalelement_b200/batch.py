@@ -174,7 +174,10 @@ class DesignMulti:
 
     ``run(classes, mode)``: classes is a list of dicts with the keyword arguments of
     `design_batch` (tensors stay alive in this object until the next run); mode 0
-    runs directly, 1 captures a CUDA graph and launches it, 2 relaunches it.
+    runs directly, 1 captures a CUDA graph and launches it, 2 relaunches it and
+    returns the outputs of the capturing call (the graph's tensors are kept for
+    as long as the graph). A mode-0 call that grows the engine's scratch makes the
+    graph stale: mode 2 then raises DOEError (capture again with mode 1).
     Returns one result dict per class, as `design_batch`.
     """
 
@@ -183,7 +186,8 @@ class DesignMulti:
         h = C.c_void_p()
         ctx.check(ctx.lib.doe_design_multi_create(ctx.h, C.byref(h)))
         self.h = h
-        self._keep = None
+        self._keep = None        # tensors of the last call
+        self._graph_keep = None  # tensors baked into the captured graph (mode 1)
 
     def close(self):
         if self.h:
@@ -199,9 +203,11 @@ class DesignMulti:
     def run(self, classes=None, mode=0):
         torch = _torch()
         if mode == 2:
+            if self._graph_keep is None:
+                raise ValueError("DesignMulti.run(mode=2): no captured graph (run mode=1 first)")
             with _Ordered(self.ctx):
                 self.ctx.check(self.ctx.lib.doe_design_multi_run(self.h, 0, None, 2))
-            return self._keep[1]
+            return self._graph_keep[1]
         descs = (_lib.DesignDevDesc * len(classes))()
         outs, keep = [], []
         for k, cl in enumerate(classes):
@@ -233,4 +239,6 @@ class DesignMulti:
         with _Ordered(self.ctx):
             self.ctx.check(self.ctx.lib.doe_design_multi_run(self.h, len(classes), descs, int(mode)))
         self._keep = (keep, outs, descs)
+        if mode == 1:  # the graph reads and writes these tensors on every relaunch
+            self._graph_keep = self._keep
         return outs

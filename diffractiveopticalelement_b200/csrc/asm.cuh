@@ -55,6 +55,8 @@ struct AsmTables {
   double* xf2;    // [nx]   fx*fx (FP64, same rounding as the reference)
   double* yf2;    // [ny]
   AsmPlane* pl;   // [nplanes]
+  float* xc;      // [nplanes][nx] the x-bin phase of xt in cycles, in [-1/2, 1/2]
+  float* yc;      // [nplanes][ny] the y-bin phase of yt in cycles
 };
 
 __device__ __forceinline__ double d_frac(double x) { return x - rint(x); }
@@ -97,6 +99,7 @@ static __global__ void asm_tables_kernel(AsmGroupArgs a, AsmTables t) {
     sincospi(2.0 * cyc, &sn, &cs);
     b.er = (float)cs;
     b.ei = (float)sn;
+    (isx ? t.xc[(long)p * a.nx + k] : t.yc[(long)p * a.ny + k]) = (float)cyc;
     double w = 1.0;
     if (a.band_limit) {
       const double lim0 = d_local_frequency_limit(n, d, lam, z);
@@ -210,14 +213,16 @@ inline int asm_tables_bytes(int nplanes, int nx, int ny, size_t* bytes) {
   b += sizeof(AxisBin) * (size_t)nplanes * nx;
   b += sizeof(AxisBin) * (size_t)nplanes * ny;
   b += sizeof(double) * (size_t)(nx + ny);
+  b += sizeof(float) * (size_t)nplanes * (nx + ny);
   b += sizeof(AsmPlane) * (size_t)nplanes + 256;
   *bytes = b;
   return 0;
 }
 
 // Layout from a 256-byte-aligned base: plane scalars (rounded to 256 B), then the
-// 16-byte AxisBin arrays, then the FP64 arrays, so every array keeps its natural
-// alignment whatever nx and ny are (including axes of length 1).
+// 16-byte AxisBin arrays, then the FP64 arrays, then the FP32 cycle arrays, so
+// every array keeps its natural alignment whatever nx and ny are (including axes
+// of length 1).
 inline AsmTables asm_tables_carve(void* base, int nplanes, int nx, int ny) {
   char* p = (char*)base;
   AsmTables t;
@@ -230,6 +235,10 @@ inline AsmTables asm_tables_carve(void* base, int nplanes, int nx, int ny) {
   t.xf2 = (double*)p;
   p += sizeof(double) * nx;
   t.yf2 = (double*)p;
+  p += sizeof(double) * ny;
+  t.xc = (float*)p;
+  p += sizeof(float) * (size_t)nplanes * nx;
+  t.yc = (float*)p;
   return t;
 }
 

@@ -75,7 +75,8 @@ extern "C" void* doe_ctx_stream(doe_ctx* c) { return c ? (void*)c->stream : null
 extern "C" int doe_ctx_synchronize(doe_ctx* c) {
   if (!c) return DOE_ERR_BAD_ARG;
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
-  return DOE_OK;
+  DOE_CUDA(c, cudaStreamSynchronize(c->aux));
+  return tc_check(c);  // a timed-out wait of an asynchronous tensor-core pass surfaces here
 }
 
 extern "C" unsigned long long doe_ctx_launch_count(doe_ctx* c) { return c ? c->launches : 0ull; }
@@ -130,6 +131,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_fused;
   } else if (k == "sweep_graph") {
     *value = c->tune_sweep_graph;
+  } else if (k == "sweep_tc") {
+    *value = c->tune_sweep_tc;
   } else {
     return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
   }
@@ -145,6 +148,10 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   }
   if (k == "sweep_graph") {
     c->tune_sweep_graph = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "sweep_tc") {
+    c->tune_sweep_tc = value ? 1 : 0;
     return DOE_OK;
   }
   if (k == "sweep_group") {

@@ -20,6 +20,7 @@ struct doe_design_multi {
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t exec = nullptr;
   unsigned long long graph_launches = 0;  // kernels inside the captured graph
+  unsigned long long graph_gen = 0;       // sub-contexts' scratch generation at capture
 };
 
 namespace {
@@ -57,6 +58,14 @@ int submit(doe_design_multi* m, int k, const doe_design_dev_desc* d, unsigned lo
   return DOE_OK;
 }
 
+// Sum of the sub-contexts' scratch generations: it changes whenever one of them
+// reallocates a slot, which leaves a captured graph pointing at freed memory.
+unsigned long long scratch_gen(const doe_design_multi* m) {
+  unsigned long long g = 0;
+  for (auto s : m->sub) g += s->slot_gen;
+  return g;
+}
+
 }  // namespace
 
 extern "C" int doe_design_multi_create(doe_ctx* c, doe_design_multi** out) {
@@ -84,12 +93,20 @@ extern "C" void doe_design_multi_destroy(doe_design_multi* m) {
 // mode 0: run directly; 1: capture the submission into a CUDA graph and launch it
 // (a mode-0 call with the same shapes must come first, so that no scratch is
 // allocated inside the capture); 2: relaunch the graph of the last mode-1 call
-// (same descriptors; the device arrays are read and written again).
+// (same descriptors; the device arrays are read and written again). A call in
+// between that grew any scratch (a mode-0 call with larger shapes) makes the
+// graph stale: mode 2 then fails with DOE_ERR_BAD_ARG instead of replaying it.
 extern "C" int doe_design_multi_run(doe_design_multi* m, int nclasses, const doe_design_dev_desc* descs, int mode) {
   if (!m) return DOE_ERR_BAD_ARG;
   doe_ctx* c = m->ctx;
   if (mode == 2) {
     if (!m->exec) return set_err(c, DOE_ERR_BAD_ARG, "design multi: no captured graph to relaunch");
+    if (scratch_gen(m) != m->graph_gen) {
+      cudaGraphExecDestroy(m->exec);
+      m->exec = nullptr;
+      return set_err(c, DOE_ERR_BAD_ARG,
+                     "design multi: the captured graph is stale (scratch was reallocated since capture); capture again");
+    }
     DOE_CUDA(c, cudaGraphLaunch(m->exec, c->stream));
     c->launches += m->graph_launches;
     return DOE_OK;
@@ -123,6 +140,7 @@ extern "C" int doe_design_multi_run(doe_design_multi* m, int nclasses, const doe
     return set_err(c, DOE_ERR_CUDA, "design multi: graph instantiation failed: %s", cudaGetErrorString(e2));
   }
   m->graph_launches = launched;
+  m->graph_gen = scratch_gen(m);
   DOE_CUDA(c, cudaGraphLaunch(m->exec, c->stream));
   c->launches += launched;
   return DOE_OK;

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -29,6 +30,8 @@ enum Slot {
   kSlotDesign0,  // design-loop state
   kSlotDesign1,
   kSlotDesign2,
+  kSlotTc,       // tensor-core FFT tables and error flag
+  kSlotTcMax,    // per-field spectrum maxima (tensor-core input scale)
   kSlotCount
 };
 
@@ -49,6 +52,10 @@ struct doe_ctx {
   cudaGraphExec_t sweep_exec = nullptr;  // graph of the last repeated device sweep
   unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
+  int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
+  void* tc_tables = nullptr;           // tensor-core tables built in this slot allocation
+  int num_sms = 0;
+  unsigned long long slot_gen = 0;     // bumped whenever a scratch slot is reallocated
   unsigned char tune_row[4][16] = {};  // chosen row-shape variant per [kind][log2 N]
   unsigned char tune_col[4][16] = {};  // chosen column-shape variant per [kind][log2 N]
   std::string err;
@@ -90,6 +97,10 @@ inline int set_err(doe_ctx* c, int code, const char* fmt, ...) {
 
 inline bool is_pow2(long n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// Reads and clears the device error flag of the tensor-core passes (prop_sweep.cu);
+// the context's streams must be synchronised.
+int tc_check(doe_ctx* c);
+
 inline int check_grid(doe_ctx* c, int nx, int ny, const char* who) {
   if (!is_pow2(nx) || !is_pow2(ny))
     return set_err(c, DOE_ERR_NOT_POW2, "%s: grid must be power-of-two, got %dx%d", who, nx, ny);
@@ -102,6 +113,7 @@ inline int check_grid(doe_ctx* c, int nx, int ny, const char* who) {
 // Ensure scratch slot s holds at least `bytes` bytes of device memory.
 inline int ensure_slot(doe_ctx* c, int s, size_t bytes, void** out) {
   if (c->slot_bytes[s] < bytes) {
+    ++c->slot_gen;  // every captured graph that baked the old address is now stale
     if (c->slot[s]) cudaFree(c->slot[s]);
     c->slot[s] = nullptr;
     c->slot_bytes[s] = 0;
@@ -207,45 +219,69 @@ inline int ilog2i(int n) {
   return l;
 }
 
+// The kernel a row / column shape launches (register-capped when MINB > 1).
+template <class S, class Op>
+inline auto row_kernel_of() {
+  if constexpr (S::MINB > 1) return row_kernel_capped<S, Op>;
+  else return row_kernel<S, Op>;
+}
+template <class S, class Op>
+inline auto col_kernel_of() {
+  if constexpr (S::MINB > 1) return col_kernel_capped<S, Op>;
+  else return col_kernel<S, Op>;
+}
+
+// One-time per-device preparation of a pass kernel: the dynamic shared-memory
+// opt-in above 48 KB. With `load` it also queries the kernel's attributes, which
+// makes a lazily loading CUDA runtime load the kernel now rather than at its
+// first launch.
+template <class K>
+inline int prepare_kernel(doe_ctx* c, K kern, int smem, std::atomic<unsigned long long>& done, bool load) {
+  const unsigned long long bit = 1ull << (c->device & 63);
+  if (smem > 48 * 1024 && !(done.load() & bit)) {
+    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done.fetch_or(bit);
+  }
+  if (load) {
+    cudaFuncAttributes fa;
+    DOE_CUDA(c, cudaFuncGetAttributes(&fa, kern));
+  }
+  return DOE_OK;
+}
+template <class S, class Op>
+inline int prepare_row(doe_ctx* c, bool load) {
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+  return prepare_kernel(c, row_kernel_of<S, Op>(), S::SMEM, attr_set, load);
+}
+template <class S, class Op>
+inline int prepare_col(doe_ctx* c, bool load) {
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+  return prepare_kernel(c, col_kernel_of<S, Op>(), S::SMEM, attr_set, load);
+}
+
 template <class S, class Op>
 inline int launch_row(doe_ctx* c, const Op& op, int nplanes, int nlines, cudaStream_t stream = nullptr) {
-  auto kern = [] {
-    if constexpr (S::MINB > 1) return row_kernel_capped<S, Op>;
-    else return row_kernel<S, Op>;
-  }();
-  static unsigned long long attr_set = 0;  // one bit per device
-  if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
-    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
-    attr_set |= 1ull << (c->device & 63);
-  }
+  DOE_TRY((prepare_row<S, Op>(c, false)));
   const long bpp = (nlines + S::V - 1) / S::V;
   const long grid = bpp * (long)nplanes;
   if (grid <= 0) return DOE_OK;
   if (grid > 0x7fffffffL) return set_err(c, DOE_ERR_UNSUPPORTED, "row pass grid too large");
   cudaStream_t st = stream ? stream : c->stream;
   LaunchScope ls(c, OpName<Op>::get(), st);
-  kern<<<(unsigned)grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, nlines);
+  row_kernel_of<S, Op>()<<<(unsigned)grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, nlines);
   DOE_CUDA(c, cudaGetLastError());
   return DOE_OK;
 }
 
 template <class S, class Op>
 inline int launch_col(doe_ctx* c, const Op& op, int nplanes, int ncols, cudaStream_t stream = nullptr) {
-  auto kern = [] {
-    if constexpr (S::MINB > 1) return col_kernel_capped<S, Op>;
-    else return col_kernel<S, Op>;
-  }();
-  static unsigned long long attr_set = 0;  // one bit per device
-  if (S::SMEM > 48 * 1024 && !(attr_set & (1ull << (c->device & 63)))) {
-    DOE_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
-    attr_set |= 1ull << (c->device & 63);
-  }
+  DOE_TRY((prepare_col<S, Op>(c, false)));
   if (nplanes <= 0) return DOE_OK;
   if (nplanes > 65535) return set_err(c, DOE_ERR_UNSUPPORTED, "column pass: at most 65535 planes per launch");
   dim3 grid((ncols + S::C - 1) / S::C, nplanes);
   cudaStream_t st = stream ? stream : c->stream;
   LaunchScope ls(c, OpName<Op>::get(), st);
-  kern<<<grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, ncols);
+  col_kernel_of<S, Op>()<<<grid, S::THREADS, S::SMEM, st>>>(op, c->tw + S::N, ncols);
   DOE_CUDA(c, cudaGetLastError());
   return DOE_OK;
 }

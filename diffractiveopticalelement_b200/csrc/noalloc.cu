@@ -19,8 +19,12 @@
 //
 // Set-up: the first call on a device resolves the array's device address with
 // cudaGetSymbolAddress (the host-side name of a __device__ array is only a
-// stand-in, not a device pointer) and fills the twiddle tables, synchronising
-// the caller's stream once. Make that first call before any stream capture.
+// stand-in, not a device pointer), fills the twiddle tables, synchronising the
+// caller's stream once, and loads every kernel this path can launch (for every
+// grid it accepts), so that a lazily loading CUDA runtime does its module loading
+// then and not inside a later call. Make that first call before any stream
+// capture. A CUDA error already pending when a call starts is reported as such
+// and left pending for its owner.
 #include <mutex>
 
 #include "ops_propagate.cuh"
@@ -35,7 +39,8 @@ constexpr size_t round_up(size_t b) { return (b + kAlign - 1) / kAlign * kAlign;
 // twiddles: table for length N at element N, N <= kMaxN (same layout as a context's)
 constexpr size_t kTwBytes = round_up(2 * (size_t)kMaxN * sizeof(float2));
 // transfer-function tables of one plane with axes up to kMaxN (asm_tables_carve layout)
-constexpr size_t kTabBytes = round_up(kAlign + 2 * (size_t)kMaxN * (sizeof(double) + sizeof(AxisBin)) + kAlign);
+constexpr size_t kTabBytes =
+    round_up(kAlign + 2 * (size_t)kMaxN * (sizeof(double) + sizeof(AxisBin) + sizeof(float)) + kAlign);
 constexpr size_t kWorkBytes = round_up((size_t)kMaxPixels * sizeof(float2));
 constexpr size_t kScratchBytes = kTwBytes + kTabBytes + kWorkBytes;  // ~2.6 MiB
 
@@ -88,6 +93,23 @@ int scratch_for_current_device(cudaStream_t stream, unsigned char** out, std::st
       *msg = std::string("doe_asm_c64_noalloc: twiddle set-up failed: ") + cudaGetErrorString(e);
       return DOE_ERR_CUDA;
     }
+    // load (and opt in to large shared memory) every pass kernel of every axis length
+    doe_ctx lc;
+    lc.device = dev;
+    cudaFuncAttributes fa;
+    int rc = cudaFuncGetAttributes(&fa, asm_tables_kernel) == cudaSuccess ? DOE_OK : DOE_ERR_CUDA;
+    for (int n = 1; n <= kMaxN && !rc; n <<= 1) {
+      rc = with_row0(n, [&](auto S) {
+        DOE_TRY((prepare_row<decltype(S), RowC64<false>>(&lc, true)));
+        return prepare_row<decltype(S), RowC64<true>>(&lc, true);
+      });
+      if (!rc) rc = with_col0(n, [&](auto S) { return prepare_col<decltype(S), ColAsm>(&lc, true); });
+    }
+    if (rc) {
+      *msg = "doe_asm_c64_noalloc: kernel set-up failed: " + (lc.err.empty() ? std::string("cudaFuncGetAttributes")
+                                                                          : lc.err);
+      return DOE_ERR_CUDA;
+    }
     g_scratch_dev[dev] = (unsigned char*)p;
   }
   *out = g_scratch_dev[dev];
@@ -100,6 +122,11 @@ extern "C" int doe_asm_c64_noalloc(const void* d_in, void* d_out, int nx, int ny
                                    double lambda, double z, int band_limit, int evanescent, double soft_edge,
                                    void* stream_handle, char* err, int err_len) {
   if (err && err_len > 0) err[0] = '\0';
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return fail(err, err_len, DOE_ERR_CUDA,
+                std::string("doe_asm_c64_noalloc: a CUDA error was pending before this call: ") +
+                    cudaGetErrorString(pending));
   if (!d_in || !d_out) return fail(err, err_len, DOE_ERR_BAD_ARG, "doe_asm_c64_noalloc: null plane");
   if (!is_pow2(nx) || !is_pow2(ny))
     return fail(err, err_len, DOE_ERR_NOT_POW2,

@@ -1,10 +1,89 @@
 // prop_sweep.cu -- batched focus sweeps (reference: src/propagate.js:427-434)
 // and the shape autotuner.
+#include <atomic>
 #include <vector>
 
 #include "ops_propagate.cuh"
+#include "tc_fft.cuh"
 
 using namespace doe;
+
+namespace {
+// Tensor-core pass set-up for this context: the B tiles and twiddle tables (built
+// once per slot allocation) and the device error flag the kernels set on a
+// timed-out wait.
+struct TcRes {
+  uint4* F;
+  float2* tw;
+  int* err;
+};
+
+int tc_prepare(doe_ctx* c, TcRes* r) {
+  void* p;
+  DOE_TRY(ensure_slot(c, kSlotTc, tcfft::kTableBytes + 256, &p));
+  r->F = (uint4*)p;
+  r->tw = (float2*)((char*)p + 2 * 16384);
+  r->err = (int*)((char*)p + tcfft::kTableBytes);
+  if (c->tc_tables != p) {
+    LaunchScope ls(c, "tc_tables");
+    tcfft::tc_tables_kernel<<<128, 128, 0, c->stream>>>(r->F, r->tw);
+    DOE_CUDA(c, cudaGetLastError());
+    DOE_CUDA(c, cudaMemsetAsync(r->err, 0, sizeof(int), c->stream));
+    c->tc_tables = p;
+  }
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+  if (!(attr_set.load() & (1ull << (c->device & 63)))) {
+    DOE_CUDA(c, cudaFuncSetAttribute(tcfft::tc_col_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     tcfft::kSmemCol));
+    DOE_CUDA(c, cudaFuncSetAttribute(tcfft::tc_row_out_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     tcfft::kSmemRow));
+    attr_set.fetch_or(1ull << (c->device & 63));
+  }
+  if (!c->num_sms) DOE_CUDA(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+  return DOE_OK;
+}
+
+// The tensor-core passes cover 1024 x 1024 planes.
+bool tc_applies(const doe_ctx* c, int nx, int ny) { return c->tune_sweep_tc && nx == tcfft::kN && ny == tcfft::kN; }
+
+// Per-field spectrum maxima (zeroed), one unsigned per field.
+int tc_maxbits(doe_ctx* c, int nfields, unsigned** out) {
+  void* p;
+  DOE_TRY(ensure_slot(c, kSlotTcMax, sizeof(unsigned) * (size_t)std::max(nfields, 1), &p));
+  DOE_CUDA(c, cudaMemsetAsync(p, 0, sizeof(unsigned) * (size_t)std::max(nfields, 1), c->stream));
+  *out = (unsigned*)p;
+  return DOE_OK;
+}
+
+int tc_absmax(doe_ctx* c, const float2* spec, long n, unsigned* maxbits) {
+  LaunchScope ls(c, "tc_absmax");
+  tcfft::absmax_kernel<<<2 * std::max(c->num_sms, 1), 256, 0, c->stream>>>(spec, n, maxbits);
+  DOE_CUDA(c, cudaGetLastError());
+  return DOE_OK;
+}
+
+// Persistent grid: `per_sm` CTAs per SM (what fits by shared memory), each taking a
+// contiguous range of tiles.
+int tc_grid(const doe_ctx* c, int ntiles, int per_sm) {
+  return std::max(1, std::min(ntiles, per_sm * std::max(c->num_sms, 1)));
+}
+}  // namespace
+
+namespace doe {
+// Reads (and clears) the tensor-core passes' device error flag; the stream must
+// be synchronised. A set flag means a bounded wait on the tensor core ran out.
+int tc_check(doe_ctx* c) {
+  if (!c->tc_tables) return DOE_OK;
+  int* err = (int*)((char*)c->tc_tables + tcfft::kTableBytes);
+  int h = 0;
+  DOE_CUDA(c, cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    DOE_CUDA(c, cudaMemset(err, 0, sizeof(int)));
+    return set_err(c, DOE_ERR_TIMEOUT, "focusSweep: a tensor-core pass gave up waiting for its MMAs (code %d)", h);
+  }
+  return DOE_OK;
+}
+}  // namespace doe
 
 // Pipelined focus sweep. Planes are processed in groups of G: the column pass of a
 // group (x H, inverse column FFT -> intermediate) runs on the context stream and
@@ -45,7 +124,10 @@ struct SweepPipe {
   // z == 0 are the input field itself (src/propagate.js:113), copied from the source.
   int run_field(const float2* spec, double dx, double dy, double lambda, const double* z, int nz, int band_limit,
                 int evanescent, double soft_edge, float2* out_c64, const float2* src_c64, double* out_re,
-                double* out_im, const double* src_re, const double* src_im) {
+                double* out_im, const double* src_re, const double* src_im, const unsigned* maxbits = nullptr) {
+    TcRes tcr{};
+    const bool use_tc = maxbits && tc_applies(c, nx, ny);
+    if (use_tc) DOE_TRY(tc_prepare(c, &tcr));
     for (int t0 = 0; t0 < nz; t0 += kMaxGroup) {  // one table launch per kMaxGroup distances
       const int tn = std::min(kMaxGroup, nz - t0);
       AsmGroupArgs a = group_args(nx, ny, dx, dy, band_limit, evanescent, soft_edge);
@@ -61,14 +143,30 @@ struct SweepPipe {
         const long o0 = (long)(t0 + g0) * pe;
         float2* w = wbuf + (g % NBUF) * (long)G * pe;
         if (g >= NBUF) DOE_CUDA(c, cudaStreamWaitEvent(c->stream, ev_row(g - NBUF), 0));
-        DOE_TRY(with_col(c, ny, kTuneSweep, [&](auto S) {
-          const ColSweepBase b{{}, spec, w, tab, nx, ny, g0};
-          if (c->tune_sweep_fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, gn, nx);
-          return launch_col<decltype(S)>(c, ColSweep{b}, gn, nx);
-        }));
+        if (use_tc) {
+          const int nt = gn * (nx / tcfft::kVec);
+          LaunchScope ls(c, "tc_sweep_col");
+          tcfft::tc_col_sweep_kernel<<<tc_grid(c, nt, 3), tcfft::kThreads, tcfft::kSmemCol, c->stream>>>(
+              tcfft::ColSweepTc{spec, w, tab, maxbits, g0}, tcr.F, tcr.tw, nt, tcr.err);
+          DOE_CUDA(c, cudaGetLastError());
+        } else {
+          DOE_TRY(with_col(c, ny, kTuneSweep, [&](auto S) {
+            const ColSweepBase b{{}, spec, w, tab, nx, ny, g0};
+            if (c->tune_sweep_fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, gn, nx);
+            return launch_col<decltype(S)>(c, ColSweep{b}, gn, nx);
+          }));
+        }
         DOE_CUDA(c, cudaEventRecord(ev_col(g), c->stream));
         DOE_CUDA(c, cudaStreamWaitEvent(c->aux, ev_col(g), 0));
-        if (out_c64) {
+        if (use_tc) {
+          const int nt = gn * (ny / tcfft::kVec);
+          LaunchScope ls(c, "tc_sweep_row", c->aux);
+          tcfft::tc_row_out_kernel<<<tc_grid(c, nt, 4), tcfft::kThreads, tcfft::kSmemRow, c->aux>>>(
+              tcfft::RowOutTc{w, out_c64 ? out_c64 + o0 : nullptr, out_c64 ? nullptr : out_re + o0,
+                              out_c64 ? nullptr : out_im + o0, maxbits, pe},
+              tcr.F, tcr.tw, nt, tcr.err);
+          DOE_CUDA(c, cudaGetLastError());
+        } else if (out_c64) {
           DOE_TRY(with_row(c, nx, kTuneSweep, [&](auto S) {
             return launch_row<decltype(S)>(c, RowC64<true>{{}, w, out_c64 + o0, nx, ny, pe, pe, 1.f / (float)pe}, gn, ny,
                                  c->aux);
@@ -127,15 +225,22 @@ extern "C" int doe_asm_sweep(doe_ctx* c, const double* re, const double* im, int
   DOE_TRY(with_col0(ny, [&](auto S) {
     return launch_col<decltype(S)>(c, ColC64<false>{{}, spec, spec, nx, ny, (long)n, (long)n, 1.f}, 1, nx);
   }));
+  unsigned* maxbits = nullptr;
+  if (tc_applies(c, nx, ny)) {
+    TcRes r;
+    DOE_TRY(tc_prepare(c, &r));
+    DOE_TRY(tc_maxbits(c, 1, &maxbits));
+    DOE_TRY(tc_absmax(c, spec, (long)n, maxbits));
+  }
   SweepPipe pipe;
   DOE_TRY(pipe.init(c, nx, ny));
   DOE_TRY(pipe.run_field(spec, dx, dy, lambda, z, nz, band_limit, evanescent, soft_edge, nullptr, nullptr, ore, oim,
-                         dre, dim));
+                         dre, dim, maxbits));
   DOE_TRY(pipe.finish());
   DOE_TRY(download_f64(c, out_re, ore, n * nz));
   DOE_TRY(download_f64(c, out_im, oim, n * nz));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
-  return DOE_OK;
+  return tc_check(c);
 }
 
 namespace {
@@ -172,7 +277,8 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
   Fnv k;
   k.val(d_fields);
   k.val(d_out);
-  for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused}) k.val(v);
+  for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused, c->tune_sweep_tc}) k.val(v);
+  k.val(c->slot_gen);  // a reallocated scratch slot invalidates the captured addresses
   for (double v : {dx, dy, soft_edge}) k.val(v);
   k.val(c->tune_sweep_group);
   k.add(c->tune_row, sizeof(c->tune_row));
@@ -231,6 +337,12 @@ int sweep_dev_body(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny
   float2* out = (float2*)d_out;
   SweepPipe pipe;
   DOE_TRY(pipe.init(c, nx, ny));
+  unsigned* maxbits = nullptr;
+  if (tc_applies(c, nx, ny)) {
+    TcRes r;
+    DOE_TRY(tc_prepare(c, &r));
+    DOE_TRY(tc_maxbits(c, nfields, &maxbits));
+  }
   for (int f = 0; f < nfields; ++f) {
     DOE_TRY(with_row(c, nx, kTuneFft, [&](auto S) {
       return launch_row<decltype(S)>(c, RowC64<false>{{}, in + f * pe, spec, nx, ny, pe, pe, 1.f}, 1, ny);
@@ -238,8 +350,10 @@ int sweep_dev_body(doe_ctx* c, const void* d_fields, int nfields, int nx, int ny
     DOE_TRY(with_col(c, ny, kTuneFft, [&](auto S) {
       return launch_col<decltype(S)>(c, ColC64<false>{{}, spec, spec, nx, ny, pe, pe, 1.f}, 1, nx);
     }));
+    if (maxbits) DOE_TRY(tc_absmax(c, spec, pe, maxbits + f));
     DOE_TRY(pipe.run_field(spec, dx, dy, lambda[f], z + (long)f * nz, nz, band_limit, evanescent, soft_edge,
-                           out + (long)f * nz * pe, in + f * pe, nullptr, nullptr, nullptr, nullptr));
+                           out + (long)f * nz * pe, in + f * pe, nullptr, nullptr, nullptr, nullptr,
+                           maxbits ? maxbits + f : nullptr));
   }
   return pipe.finish();
 }
@@ -387,7 +501,8 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     c->tune_col[kind][ly] = (unsigned char)pick[kind == kTuneFft ? 1 : 3];
     if (kind == kTuneSweep) c->tune_sweep_fused = best_f;
   }
-  // planes per launch pair of the pipelined sweep: time one 64-distance field
+  // planes per launch pair of the pipelined sweep, and (for 1024^2 planes) the
+  // tensor-core passes against the CUDA-core passes: time one 64-distance field
   {
     const int nz = 64;
     std::vector<double> zs(nz);
@@ -396,24 +511,42 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     DOE_TRY(ensure_slot(c, kSlotOut, (size_t)nz * pe * sizeof(float2), &dout));
     float best = 1e30f;
     long bestG = 0;
+    int bestTc = 0;
     const long saved = c->tune_sweep_group;
-    for (long G : {4L, 8L, 16L, 32L, 64L}) {
-      if ((size_t)G * pe * sizeof(float2) * SweepPipe::NBUF > ((size_t)1 << 31)) break;
-      c->tune_sweep_group = G;
-      float ms;
-      DOE_TRY((c->tune_sweep_graph ? time_graph : time_variant)(c, [&]() {
-        SweepPipe pipe;
-        DOE_TRY(pipe.init(c, nx, ny));
-        DOE_TRY(pipe.run_field(spec, dx, dy, lambda, zs.data(), nz, 1, 1, 0.02, (float2*)dout, spec, nullptr,
-                               nullptr, nullptr, nullptr));
-        return pipe.finish();
-      }, &ms));
-      if (ms < best) {
-        best = ms;
-        bestG = G;
+    const int tc_allowed = c->tune_sweep_tc;
+    for (int tc : {1, 0}) {
+      c->tune_sweep_tc = tc;
+      if (tc && !(tc_allowed && tc_applies(c, nx, ny))) continue;
+      unsigned* mb = nullptr;
+      if (tc) {
+        TcRes r;
+        DOE_TRY(tc_prepare(c, &r));
+        DOE_TRY(tc_maxbits(c, 1, &mb));
+        DOE_TRY(tc_absmax(c, spec, pe, mb));
+      }
+      for (long G : {2L, 4L, 8L, 16L, 32L, 64L}) {
+        if ((size_t)G * pe * sizeof(float2) * SweepPipe::NBUF > ((size_t)1 << 31)) break;
+        if (!tc && G < 4) continue;
+        c->tune_sweep_group = G;
+        float ms;
+        DOE_TRY((c->tune_sweep_graph ? time_graph : time_variant)(c, [&]() {
+          SweepPipe pipe;
+          DOE_TRY(pipe.init(c, nx, ny));
+          DOE_TRY(pipe.run_field(spec, dx, dy, lambda, zs.data(), nz, 1, 1, 0.02, (float2*)dout, spec, nullptr,
+                                 nullptr, nullptr, nullptr, mb));
+          return pipe.finish();
+        }, &ms));
+        if (ms < best) {
+          best = ms;
+          bestG = G;
+          bestTc = tc;
+        }
       }
     }
+    c->tune_sweep_tc = bestTc;
     c->tune_sweep_group = saved > 0 ? saved : bestG;
+    DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+    DOE_TRY(tc_check(c));
   }
   if (chosen) {
     for (int k = 0; k < 4; ++k) chosen[k] = pick[k];

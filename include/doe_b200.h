@@ -73,17 +73,21 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
 /* Tuning knobs (engine-only): "sweep_group" = planes per focus-sweep launch pair
  * (0 = sized from the L2 cache); "sweep_fused" = 1 to read and multiply per
  * element in the sweep column pass (0: all reads first); "sweep_graph" = 0 to
- * disable CUDA-graph replay of repeated device sweeps; "fft_row", "fft_col",
+ * disable CUDA-graph replay of repeated device sweeps; "sweep_tc" = 0 to run
+ * 1024 x 1024 focus sweeps on the FP32 CUDA-core passes instead of the tcgen05
+ * tensor-core passes (default 1); "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
-/* Current value of "sweep_group", "sweep_fused" or "sweep_graph". */
+/* Current value of "sweep_group", "sweep_fused", "sweep_graph" or "sweep_tc". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for
  * the plain FFT and focus-sweep passes, then times the pipelined sweep for
- * several group sizes ("sweep_group"). chosen (5 ints, may be NULL) receives the
- * picked {fft row, fft column, sweep row, sweep column} variants and group size. */
+ * several group sizes ("sweep_group") on the CUDA-core passes and, for 1024^2
+ * grids with "sweep_tc" on, on the tensor-core passes, keeping the fastest pair
+ * ("sweep_tc", "sweep_group"). chosen (5 ints, may be NULL) receives the picked
+ * {fft row, fft column, sweep row, sweep column} variants and group size. */
 int doe_autotune(doe_ctx* ctx, int nx, int ny, double dx, double dy, double lambda, double z,
                  int* chosen);
 

@@ -345,6 +345,24 @@ def test_uneven_sizes_in_one_submission_and_graph_relaunch(engine, oracle):
         for r, o in zip(ref, outs):
             assert torch.equal(r["phase"], o["phase"]), mode
             assert torch.equal(r["error"], o["error"]), mode
+    # a direct call with the same shapes leaves the graph valid: the relaunch
+    # rewrites the captured call's tensors, not those of the direct call
+    m.run(classes, 0)
+    for cl, p0 in zip(classes, ph0):
+        cl["phase"].copy_(p0)
+    outs = m.run(None, 2)
+    torch.cuda.synchronize()
+    for r, o in zip(ref, outs):
+        assert torch.equal(r["phase"], o["phase"])
+    # a direct call that grows the scratch (a larger class) makes the graph stale
+    n = 512
+    ill = oracle.disc_mask(n, n, DX, DX, 0.45 * n * DX, 2 * DX)
+    big = dict(classes[0], nx=n, illumination=f(ill), target_amp=f([oracle.prepare_target(disc(n, 60), ill)] * 8),
+               roi=f([oracle.auto_roi(disc(n, 60), n, n)] * 8), phase=f(np.zeros((8, n * n))))
+    m.run(classes + [big], 0)
+    from diffractiveopticalelement_b200 import DOEError
+    with pytest.raises(DOEError, match="stale"):
+        m.run(None, 2)
     m.close()
 
 
