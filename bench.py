@@ -39,6 +39,25 @@ NFIELDS, NZ = 64, 64
 DX = 4e-6
 LAMBDAS = (450e-9, 532e-9, 633e-9)
 BYTES_PER_PX = 16  # read complex64 spectrum + write complex64 output, per output plane
+# profiler labels of the two focus-sweep passes (CUDA-core and tensor-core forms)
+SWEEP_PASSES = {"asm_sweep_col": "column", "tc_sweep_col": "column", "fft_row_inv": "row", "tc_sweep_row": "row"}
+
+
+def recorded_traffic(kernel, planes_per_launch):
+    """DRAM bytes of one launch of `kernel` (this many planes) from the committed
+    ncu capture record: rows `| kernel | dram bytes per plane | ... |` of
+    profiles/traffic_sweep_1024.md; None when the kernel has no record."""
+    path = os.path.join(ROOT, "profiles", "traffic_sweep_1024.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 2 and cells[0] == f"`{kernel}`":
+            try:
+                return float(cells[1]) * planes_per_launch
+            except ValueError:
+                return None
+    return None
 METRIC = "1024^2 ASM props/s (batched band-limited focus sweep)"
 CONFIG = {"workload": "asm_focus_sweep", "fields": NFIELDS, "distances_per_field": NZ, "grid": [NX, NY],
           "pitch_um": DX * 1e6, "lambda_nm": [450, 532, 633], "z_mm": [15, 48], "band_limit": True,
@@ -164,44 +183,92 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def main_wgs(args, ctx, device, rank, world, local):
-    """--workload wgs256: batched image-plane WGS designs/s to screen RMSE <= 1%."""
+# Algorithmic bytes per pixel of each design pass: the complex64 work plane read
+# and written (16 B) plus the FP32 side planes the pass must read or write.
+PASS_BYTES_PX = {
+    "design_col_fwd": 24, "design_col_back": 24,              # + the tabulated transfer function (8 B)
+    "design_row_wgs_first": 32, "design_row_wgs_target": 32,  # W in, U out, t, m in, w in/out
+    "design_row_wgs_constrain": 28,                           # U in, t, m, w in, W out
+    "design_row_doe_update": 24, "design_row_doe_last": 16,   # W in/out, A in, phase out
+    "design_row_doe_fwd": 16,                                 # A, phase in, W out
+    "design_col_fourier": 28, "design_col_fourier_wgs": 36,   # W in/out, t, m in, amplitude out (+ w in/out)
+    "design_row_gs_target": 24, "design_row_gs_final": 20,    # W in/out, t, m in (final: amplitude out)
+}
+
+
+def kernel_roofline(prof, px_per_launch, table=None):
+    """Roofline of the dominant kernel of a profiled step (each launch timed alone
+    between CUDA events on its stream): its algorithmic bytes per launch (bytes
+    per pixel x pixels per launch) over its average launch time."""
+    table = PASS_BYTES_PX if table is None else table
+    known = {k: v for k, v in prof.items() if k in table and v[1] > 0}
+    if not known:
+        return None
+    peak, peak_kind = peaks()
+    name, (tot_ms, cnt) = max(known.items(), key=lambda kv: kv[1][0])
+    avg_s = tot_ms / cnt / 1e3
+    bpl = table[name] * px_per_launch
+    ach = bpl / avg_s / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_kind": peak_kind, "bytes_per_px": table[name], "bytes_per_launch": bpl,
+            "avg_launch_us": avg_s * 1e6, "launches": cnt, "traffic": None,
+            "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()}}
+
+
+WGS_CONFIG = {"workload": "wgs256", "grid": [256, 256], "max_iterations": 100,
+              "goal": "screen RMSE <= 1% (src/projector.js:554-595)", "pitch_um": 8, "lambda_nm": 532, "z_mm": 30,
+              "illumination": "rect, 0.9 N dx, raised-cosine edge 2 dx (src/doe.js:979-1000)",
+              "targets": "3-8 seeded rectangles 4-40 px in the central 128^2, autoRoi", "band_limit": False}
+
+
+def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=0, world=1):
+    """C1 (plain GPU WGS to the goal) and C4 (surrogate warm start + WGS to the goal)
+    on the same seeded designs, the fixed 100-iteration loop (all designs active,
+    profiled for the per-kernel roofline), and the CPU port on all host threads and
+    on one."""
     import torch
     import torch.distributed as dist
+    r = run_wgs(ctx, device, designs, max(warmup, 3), steps, goal=0.01, rank=rank)
+    fixed = run_wgs(ctx, device, designs, 1, 1, rank=rank)
+    ms, reached = r["ms_per_step"], r["reached"]
+    if world > 1:
+        t = torch.tensor([ms, reached], dtype=torch.float64, device=device)
+        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms, reached = float(t[0].item()), int(t[1].item())
+    r.pop("_used")
+    roof = kernel_roofline(fixed.pop("_prof"), designs * WGS_N * WGS_N)
+    r.pop("_prof", None)
+    if roof:
+        roof["basis"] = ("dominant pass of the fixed 100-iteration loop (every design active): bytes per pixel x "
+                         "designs x 256^2 over its average launch time")
+    out = {"metric": WGS_METRIC, "value": reached / (ms / 1e3), "unit": "designs/s", "ms_per_step": ms,
+           "config": dict(WGS_CONFIG, designs=designs), "roofline": roof, "wgs256": r,
+           "fixed_100_iterations": fixed, "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
+    if surrogate_steps > 0:
+        warm = run_warm(ctx, device, designs, surrogate_steps)
+        warm["vs_plain"] = warm["designs_per_s"] / out["value"] if out["value"] else None
+        out["surrogate_warm_start"] = warm
+    out["cpu_baseline"] = wgs_cpu_baseline() if cpu else None
+    if cpu:
+        one = wgs_cpu_baseline(n_designs=2, threads=1)
+        out["cpu_baseline"]["single_core"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
+    return out
+
+
+def main_wgs(args, ctx, device, rank, world, local):
+    """--workload wgs256: batched image-plane WGS designs/s to screen RMSE <= 1%."""
     sampler = ClockSampler(local)
     steps = max(1, args.steps if args.steps != 20 else 3)
     sampler.start()
-    r = run_wgs(ctx, device, args.designs, max(args.warmup, 3), steps, goal=0.01, rank=rank)
+    body = measure_wgs(ctx, device, args.designs, args.warmup, steps, args.surrogate_steps,
+                       rank == 0 and world == 1 and not args.no_cpu_baseline, rank, world)
     clocks = sampler.stop()
-    fixed = run_wgs(ctx, device, args.designs, 1, 1, rank=rank)
-    ms = r["ms_per_step"]
-    reached = r["reached"]
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        t = torch.tensor([reached], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        reached = int(t.item())
-    value = reached / (ms / 1e3)
-    r.pop("_used")
-    warm = run_warm(ctx, device, args.designs, args.surrogate_steps) if args.surrogate_steps > 0 else None
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = wgs_cpu_baseline()
     if rank == 0:
-        line = {"metric": WGS_METRIC, "value": value,
-                "unit": "designs/s", "n_gpus": world, "steps": steps, "warmup": max(args.warmup, 3),
-                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "fp32 fields, fp64 reductions", "data": "synthetic",
-                "config": {"workload": "wgs256", "designs": args.designs, "grid": [WGS_N, WGS_N],
-                           "max_iterations": WGS_ITERS, "goal": "screen RMSE <= 1% (src/projector.js:554-595)",
-                           "pitch_um": 8, "lambda_nm": 532, "z_mm": 30,
-                           "targets": "3-8 seeded rectangles 4-40 px in the central 128^2", "band_limit": False,
-                           "l2_flush": f"{args.designs} designs x 4 MiB of state exceed L2"},
-                "clocks": clocks, "wgs256": r, "fixed_100_iterations": fixed, "surrogate_warm_start": warm,
-                "cpu_baseline": cpu, "e2e": None,
-                "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
+        line = dict(body, n_gpus=world, steps=steps, warmup=max(args.warmup, 3), higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="fp32 fields, fp64 reductions", data="synthetic",
+                    clocks=clocks, e2e=None)
+        line["config"]["l2_flush"] = f"{args.designs} designs x 4 MiB of state exceed L2"
         print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -229,12 +296,12 @@ def mp_inputs(n=MP_N, B=MP_B):
     return ill, irr, tgt, roi
 
 
-def mp_cpu_baseline(iters=1):
+def mp_cpu_baseline(iters=1, threads=None):
     """Oracle multi-plane GS at 2048^2: one design per host thread for `iters`
     iterations (the full 100 would take minutes per design); design-iterations/s."""
     from oracle import oracle as O
     O.build()
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     nd = threads
     ill, irr, tgt, roi = mp_inputs(B=1)
 
@@ -252,8 +319,8 @@ def mp_cpu_baseline(iters=1):
                       f"FP64 C restatement of gerchbergSaxtonMultiPlane (no JS runtime on this box)"}
 
 
-def main_multiplane(args, ctx, device, rank, world, local):
-    """--workload multiplane2048: batched 4 x 2048^2 three-plane GS."""
+def measure_multiplane(ctx, device, warmup, steps, cpu, e2e_on, rank=0, world=1):
+    """C5: batched 4 x 2048^2 three-plane GS, 100 iterations from a flat start."""
     import torch
     import torch.distributed as dist
     import diffractiveopticalelement_b200 as E
@@ -271,13 +338,9 @@ def main_multiplane(args, ctx, device, rank, world, local):
         res["r"] = batch.multiplane_batch(ctx, d_ill, d_tgt, d_ph, list(MP_Z), nx=MP_N, ny=MP_N, dx=MP_DX,
                                           lam=MP_LAM, iterations=MP_ITERS, roi=d_roi)
 
-    steps = max(1, args.steps if args.steps != 20 else 2)
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         step()
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
     if world > 1:
         dist.barrier()
     n0 = ctx.lib.doe_ctx_launch_count(ctx.h)
@@ -288,7 +351,6 @@ def main_multiplane(args, ctx, device, rank, world, local):
     e1.record()
     e1.synchronize()
     launches = int(ctx.lib.doe_ctx_launch_count(ctx.h) - n0)
-    clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / steps
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=device)
@@ -301,13 +363,15 @@ def main_multiplane(args, ctx, device, rank, world, local):
     prof = profile_read(None, ctx)
     ctx.lib.doe_ctx_set_profiling(ctx.h, 0)
     peak, peak_kind = peaks()
-    # 6 propagations per iteration x 16 B/px (read + write complex64)
-    alg_bytes = 96.0 * n * MP_B * MP_ITERS
-    achieved = alg_bytes / (ms / 1e3) / 1e9
+    roof = kernel_roofline(prof, MP_B * n)
+    if roof:
+        roof["basis"] = "dominant pass: bytes per pixel x 4 designs x 2048^2 over its average launch time"
+        alg = 96.0 * n * MP_B * MP_ITERS  # 6 propagations per iteration x 16 B/px
+        roof["whole_loop"] = {"achieved": alg / (ms / 1e3) / 1e9, "frac": alg / (ms / 1e3) / 1e9 / peak,
+                              "basis": "96 B/px per iteration (6 propagations x 16 B/px)"}
     err = res["r"]["error"][:, -1].cpu().numpy()
-    # e2e: one design through the host-buffer call (FP64 planes, copies inside the region)
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if e2e_on:  # one design through the host-buffer call (FP64 planes, copies inside the region)
         planes = [{"z": MP_Z[p], "targetAmp": tgt[0, p], "roi": roi[0, p]} for p in range(P)]
         o = {"nx": MP_N, "dx": MP_DX, "lambda": MP_LAM, "iterations": MP_ITERS}
         E.gerchbergSaxtonMultiPlane(ill, planes, dict(o, iterations=2))
@@ -317,18 +381,29 @@ def main_multiplane(args, ctx, device, rank, world, local):
         e2e = {"value": MP_ITERS / dt, "unit": "design-iterations/s", "h2d_bytes_per_step": (2 + 2 * P) * n * 8,
                "d2h_bytes_per_step": n * 8,
                "sample": "design 0 through gerchbergSaxtonMultiPlane (doe_multiplane, FP64 host planes)"}
-    cpu = mp_cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    cb = None
+    if cpu:
+        cb = mp_cpu_baseline()
+        one = mp_cpu_baseline(threads=1)
+        cb["single_core"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
+    return {"metric": MP_METRIC, "value": value, "unit": "design-iterations/s", "ms_per_step": ms,
+            "config": MP_CONFIG, "roofline": roof,
+            "final_error": {"median": float(np.median(err)), "max": float(err.max())},
+            "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches}
+
+
+def main_multiplane(args, ctx, device, rank, world, local):
+    """--workload multiplane2048: batched 4 x 2048^2 three-plane GS."""
+    steps = max(1, args.steps if args.steps != 20 else 2)
+    sampler = ClockSampler(local)
+    sampler.start()
+    body = measure_multiplane(ctx, device, args.warmup, steps, rank == 0 and world == 1 and not args.no_cpu_baseline,
+                              rank == 0 and not args.no_e2e, rank, world)
+    clocks = sampler.stop()
     if rank == 0:
-        line = {"metric": MP_METRIC, "value": value, "unit": "design-iterations/s", "n_gpus": world, "steps": steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "fp32 fields, fp64 reductions", "data": "synthetic",
-                "config": MP_CONFIG, "clocks": clocks,
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                             "basis": "96 B/px per iteration (6 propagations x 16 B/px), whole loop",
-                             "per_kernel_ms": {k: round(v[0], 3) for k, v in prof.items()}},
-                "final_error": {"median": float(np.median(err)), "max": float(err.max())},
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches}
+        line = dict(body, n_gpus=world, steps=steps, warmup=max(args.warmup, 3), higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="fp32 fields, fp64 reductions", data="synthetic",
+                    clocks=clocks)
         print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -378,7 +453,8 @@ def uneven_inputs(sizes):
 
 def uneven_cpu_baseline(iters=2):
     """Oracle fourierCgh: one design per size for `iters` iterations on one thread,
-    extrapolated to the workload (counts x 200 iterations) over all host threads."""
+    extrapolated to the workload (counts x 200 iterations) over all host threads
+    (and over one)."""
     from oracle import oracle as O
     O.build()
     sizes = uneven_specs()
@@ -392,14 +468,17 @@ def uneven_cpu_baseline(iters=2):
         per_iter[n] = (time.perf_counter() - t0) / iters
     threads = os.cpu_count() or 1
     t1 = sum(per_iter[n] * UN_ITERS for n in sizes)
+    timing = ", ".join(f"{n}^2: {1e3 * per_iter[n]:.1f} ms/it" for n in UN_SIZES)
     return {"value": UN_COUNT / (t1 / threads), "unit": "designs/s", "cores": threads, "kind": "port",
             "sample": f"one design per size x {iters} iterations of the FP64 C restatement of fourierCgh on one "
-                      f"thread ({', '.join(f'{n}^2: {1e3 * per_iter[n]:.1f} ms/it' for n in UN_SIZES)}), "
-                      f"extrapolated to the 512-design, 200-iteration workload over {threads} threads"}
+                      f"thread ({timing}), extrapolated to the 512-design, 200-iteration workload over {threads} "
+                      f"threads",
+            "single_core": {"value": UN_COUNT / t1, "cores": 1,
+                            "sample": "the same per-iteration timings extrapolated to one thread"}}
 
 
-def main_uneven(args, ctx, device, rank, world, local):
-    """--workload farfield_uneven: 512 far-field GS designs of four sizes in one CUDA-graph launch."""
+def measure_uneven(ctx, device, warmup, steps, cpu, rank=0, world=1):
+    """C3: 512 far-field GS designs of four sizes in one CUDA-graph launch."""
     import torch
     import torch.distributed as dist
     from diffractiveopticalelement_b200 import batch
@@ -422,25 +501,20 @@ def main_uneven(args, ctx, device, rank, world, local):
     reset()
     m.run(classes, 0)  # sizes the scratch of every class
     torch.cuda.synchronize()
-    # direct submission (no graph), for comparison
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reset()
     e0.record()
-    m.run(classes, 0)
+    m.run(classes, 0)  # direct submission (no graph), for comparison
     e1.record()
     e1.synchronize()
     ms_direct = e0.elapsed_time(e1)
     reset()
     m.run(classes, 1)  # capture + launch
     torch.cuda.synchronize()
-    steps = max(1, args.steps if args.steps != 20 else 3)
-    for _ in range(max(args.warmup, 3) - 1):
+    for _ in range(max(warmup, 3) - 1):
         reset()
         m.run(None, 2)
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
     if world > 1:
         dist.barrier()
     n0 = ctx.lib.doe_ctx_launch_count(ctx.h)
@@ -451,35 +525,48 @@ def main_uneven(args, ctx, device, rank, world, local):
     e1.record()
     e1.synchronize()
     launches = int(ctx.lib.doe_ctx_launch_count(ctx.h) - n0)
-    clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / steps
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = UN_COUNT * world / (ms / 1e3)
-    counts = {n: sum(1 for s in sizes if s == n) for n in UN_SIZES}
+    counts = {n: sum(1 for s_ in sizes if s_ == n) for n in UN_SIZES}
     flops = sum(c * 10.0 * n * n * np.log2(n * n) * UN_ITERS for n, c in counts.items())
-    bytes_ = sum(c * 32.0 * n * n * UN_ITERS for n, c in counts.items())
+    per_iter_px = PASS_BYTES_PX["design_col_fourier"] + PASS_BYTES_PX["design_row_doe_update"]
+    bytes_ = sum(c * float(per_iter_px) * n * n * UN_ITERS for n, c in counts.items())
     peak, peak_kind = peaks()
     err = np.concatenate([o["error"][:, -1].cpu().numpy() for o in outs])
-    cpu = uneven_cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
-    if rank == 0:
-        line = {"metric": UN_METRIC, "value": value, "unit": "designs/s", "n_gpus": world, "steps": steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "fp32 fields, fp64 reductions", "data": "synthetic",
-                "config": dict(UN_CONFIG, counts={str(k): v for k, v in counts.items()}), "clocks": clocks,
-                "roofline": {"bound": "hbm", "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                             "frac": bytes_ / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
-                             "basis": "32 B/px per iteration (two FFT passes x 16 B/px), all designs",
-                             "fft_tflops": flops / (ms / 1e3) / 1e12,
-                             "fft_basis": "10 N^2 log2(N^2) FLOP per iteration"},
-                "graph": {"ms_per_step_graph": ms, "ms_per_step_direct": ms_direct,
-                          "kernels_per_step": launches / steps},
-                "final_error": {"median": float(np.median(err)), "max": float(err.max())},
-                "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches}
-        print(json.dumps(line), flush=True)
+    cb = uneven_cpu_baseline() if cpu else None
     m.close()
+    return {"metric": UN_METRIC, "value": value, "unit": "designs/s", "ms_per_step": ms,
+            "config": dict(UN_CONFIG, counts={str(k): v for k, v in counts.items()}),
+            "roofline": {"bound": "hbm", "kernel": "whole graph (column + row pass per iteration, all classes)",
+                         "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bytes_ / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                         "basis": f"{per_iter_px} B/px per iteration (far-field column pass "
+                                  f"{PASS_BYTES_PX['design_col_fourier']} + row pass "
+                                  f"{PASS_BYTES_PX['design_row_doe_update']}), all designs, over the graph's time",
+                         "fft_tflops": flops / (ms / 1e3) / 1e12,
+                         "fft_basis": "10 N^2 log2(N^2) FLOP per iteration"},
+            "graph": {"ms_per_step_graph": ms, "ms_per_step_direct": ms_direct, "kernels_per_step": launches / steps},
+            "final_error": {"median": float(np.median(err)), "max": float(err.max())},
+            "cpu_baseline": cb, "e2e": None, "gpu_launches": launches}
+
+
+def main_uneven(args, ctx, device, rank, world, local):
+    """--workload farfield_uneven: 512 far-field GS designs of four sizes in one CUDA-graph launch."""
+    steps = max(1, args.steps if args.steps != 20 else 3)
+    sampler = ClockSampler(local)
+    sampler.start()
+    body = measure_uneven(ctx, device, args.warmup, steps, rank == 0 and world == 1 and not args.no_cpu_baseline,
+                          rank, world)
+    clocks = sampler.stop()
+    if rank == 0:
+        line = dict(body, n_gpus=world, steps=steps, warmup=max(args.warmup, 3), higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="fp32 fields, fp64 reductions", data="synthetic",
+                    clocks=clocks)
+        print(json.dumps(line), flush=True)
     ctx.close()
     return 0
 
@@ -618,13 +705,14 @@ def wgs_inputs(n_designs, seed0=1):
     return ill, np.array(irr), np.array(roi), np.array(tgt), np.array(ph)
 
 
-def wgs_cpu_baseline(n_designs=None, iters=WGS_ITERS, goal=0.01):
-    """Oracle WGS designs on all host threads (one design per thread), each stopped
-    at the first iteration whose screen RMSE is <= goal (at most `iters`), the same
-    rule as the GPU arm. Returns the rate of designs that met the goal."""
+def wgs_cpu_baseline(n_designs=None, iters=WGS_ITERS, goal=0.01, threads=None):
+    """Oracle WGS designs on `threads` host threads (default all; one design per
+    thread), each stopped at the first iteration whose screen RMSE is <= goal (at
+    most `iters`), the same rule as the GPU arm. Returns the rate of designs that
+    met the goal."""
     from oracle import oracle as O
     O.build()
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     nd = n_designs or threads
     ill, irr, roi, tgt, ph = wgs_inputs(nd, seed0=1)
     used, ok = [0] * nd, [False] * nd
@@ -654,7 +742,7 @@ def wgs_cpu_baseline(n_designs=None, iters=WGS_ITERS, goal=0.01):
     dt = time.perf_counter() - t0
     return {"value": sum(ok) / dt, "unit": "designs/s", "cores": threads, "kind": "port",
             "sample": f"{nd} designs of 256^2 WGS (seeds 1-{nd}) to screen RMSE <= {goal:g} (median "
-                      f"{int(np.median(used))} iterations, {sum(ok)} met it), one design per thread, FP64 C "
+                      f"{int(np.median(used))} iterations, {sum(ok)} met it) on {threads} thread(s), FP64 C "
                       f"restatement of weightedGerchbergSaxton (no JS runtime on this box)"}
 
 
@@ -706,7 +794,7 @@ def run_wgs(ctx, device, n_designs, warmup, steps, goal=0.0, iters=WGS_ITERS, ra
            "screen_rmse": {"median": float(np.median(rm)), "min": float(rm.min()), "max": float(rm.max()),
                            "le_1pct": int(np.sum(rm <= 0.01))},
            "efficiency_median": float(np.median(met[:, 1])), "gpu_launches_per_step": launches / steps,
-           "per_kernel_ms": {k: round(v[0], 3) for k, v in prof.items()}}
+           "per_kernel_ms": {k: round(v[0], 3) for k, v in prof.items()}, "_prof": prof}
     if goal:
         out.update({"goal": goal, "reached": reached,
                     "iterations_used": {"median": float(np.median(used)), "min": int(used.min()),
@@ -788,6 +876,8 @@ def main():
     ap.add_argument("--workload", default="sweep", choices=["sweep", "wgs256", "multiplane2048", "farfield_uneven"])
     ap.add_argument("--designs", type=int, default=1024, help="designs per step of the WGS workload")
     ap.add_argument("--no-wgs", action="store_true", help="skip the WGS block of the default line")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the WGS, uneven far-field and multi-plane keys")
     ap.add_argument("--surrogate-steps", type=int, default=1500,
                     help="training steps of the warm-start surrogate in the wgs256 workload (0: skip the warm arm)")
     ap.add_argument("--pin-tuning", default=None,
@@ -897,34 +987,35 @@ def main():
     props = nfields * NZ * args.steps * world
     value = props / (ms / 1000.0)
 
-    # ---- per-kernel durations (instrumented step right after the timed region)
+    # ---- per-kernel durations: one instrumented step right after the timed region,
+    # with the two passes serialised on one stream so that each launch is timed alone
     L.doe_ctx_set_profiling(ctx.h, 1)
     step()
     prof = profile_read(E, ctx)
     L.doe_ctx_set_profiling(ctx.h, 0)
     peak, peak_kind = peaks()
-    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else None
     roofline = None
-    if dom:
-        name, (tot_ms, cnt) = dom
+    sweep_kernels = {k: v for k, v in prof.items() if k in SWEEP_PASSES}
+    if sweep_kernels:
+        name, (tot_ms, cnt) = max(sweep_kernels.items(), key=lambda kv: kv[1][0])
+        planes_per_launch = nfields * NZ / cnt
         # column pass: the spectrum once per launch + every intermediate plane written
         # (8 B/px each); row pass: read intermediate + write output (16 B/px per plane)
-        planes_per_launch = nfields * NZ / cnt
-        if name == "asm_sweep_col":
+        if SWEEP_PASSES[name] == "column":
             bytes_per_launch = (planes_per_launch + 1) * NX * NY * 8
         else:
             bytes_per_launch = planes_per_launch * NX * NY * 16
         avg_s = tot_ms / cnt / 1000.0
         achieved = bytes_per_launch / avg_s / 1e9
-        # DRAM bytes of one full-size sweep column launch (64 planes), ncu capture in
-        # profiles/asm_sweep_col_1024.md; other kernels have no full-size capture
-        traffic = 517.09e6 * planes_per_launch / 64 if name == "asm_sweep_col" else None
+        traffic = recorded_traffic(name, planes_per_launch)
         roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch",
-                    "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6,
-                    "launches": cnt,
-                    "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()}}
+                    "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at "
+                                       "full size, per plane, scaled to this launch's planes "
+                                       "(profiles/traffic_sweep_1024.md)") if traffic else None,
+                    "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6, "launches": cnt,
+                    "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()},
+                    "per_kernel_note": "instrumented step with both passes on one stream (each launch timed alone)"}
         sweep_bytes = nfields * NZ * NX * NY * BYTES_PER_PX
         roofline["sweep_frac"] = (sweep_bytes / (ms / 1000.0 / args.steps) / 1e9) / peak
 
@@ -971,26 +1062,34 @@ def main():
         host_fields = fields[:4].cpu().numpy()
         nplanes = threads * 2
         t = cpu_sample(params, host_fields, nplanes, threads)
+        t1 = cpu_sample(params, host_fields, 2, 1)
         cpu = {"value": nplanes / t, "unit": "props/s", "cores": threads, "kind": "port",
                "sample": f"{nplanes} band-limited 1024^2 propagations of the workload (fields 0-3) on {threads} "
-                         f"threads, FP64 C restatement of propagateAngularSpectrum (no JS runtime on this box)"}
+                         f"threads, FP64 C restatement of propagateAngularSpectrum (no JS runtime on this box)",
+               "single_core": {"value": 2 / t1, "cores": 1,
+                               "sample": "2 propagations of the workload on one thread (the reference is "
+                                         "single-threaded JavaScript)"}}
 
-    wgs = None
-    if rank == 0 and not args.no_wgs:
+    # ---- the other configurations, as keys of the same line (one GPU only)
+    extras = {}
+    if world == 1 and not args.no_extras:
         del out
         out = None
         torch.cuda.empty_cache()
-        wgs = run_wgs(ctx, device, min(args.designs, 512), 1, 2, goal=0.01)
-        wgs.pop("_used", None)
-        wgs["note"] = ("secondary workload (256^2 image-plane WGS to screen RMSE <= 1%, at most 100 iterations, "
-                       "seeded rectangle targets); bench.py --workload wgs256 makes it the primary line")
+        cpu_on = not args.no_cpu_baseline
+        if not args.no_wgs:
+            extras["wgs256"] = measure_wgs(ctx, device, 512, 1, 2, args.surrogate_steps, cpu_on)
+        torch.cuda.empty_cache()
+        extras["farfield_uneven"] = measure_uneven(ctx, device, 1, 2, cpu_on)
+        torch.cuda.empty_cache()
+        extras["multiplane2048"] = measure_multiplane(ctx, device, 1, 2, cpu_on, False)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32), fp64 phase reduction",
                 "data": "synthetic", "config": dict(CONFIG, fields=nfields, tuned_variants=tuned), "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "wgs256": wgs}
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, **extras}
         print(json.dumps(line), flush=True)
     del out, fields
     ctx.close()

@@ -35,13 +35,22 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
+def _includes(path: str, seen: set) -> set:
+    """Every file reachable through #include "..." from `path` (quoted includes only)."""
+    import re
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', open(path).read(), re.M):
+        _includes(os.path.normpath(os.path.join(os.path.dirname(path), name)), seen)
+    return seen
+
+
 def _stale(obj: str, src: str) -> bool:
     if not os.path.exists(obj):
         return True
     t = os.path.getmtime(obj)
-    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
-    deps.append(os.path.join(os.path.dirname(HERE), "include", "doe_b200.h"))
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(os.path.getmtime(d) > t for d in _includes(src, set()))
 
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:

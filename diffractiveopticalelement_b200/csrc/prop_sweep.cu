@@ -34,9 +34,9 @@ int tc_prepare(doe_ctx* c, TcRes* r) {
   static std::atomic<unsigned long long> attr_set{0};  // one bit per device
   if (!(attr_set.load() & (1ull << (c->device & 63)))) {
     DOE_CUDA(c, cudaFuncSetAttribute(tcfft::tc_col_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     tcfft::kSmemCol));
+                                     tcfft::kSmemBytes));
     DOE_CUDA(c, cudaFuncSetAttribute(tcfft::tc_row_out_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     tcfft::kSmemRow));
+                                     tcfft::kSmemBytes));
     attr_set.fetch_or(1ull << (c->device & 63));
   }
   if (!c->num_sms) DOE_CUDA(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -128,6 +128,9 @@ struct SweepPipe {
     TcRes tcr{};
     const bool use_tc = maxbits && tc_applies(c, nx, ny);
     if (use_tc) DOE_TRY(tc_prepare(c, &tcr));
+    // With launch profiling on, both passes run on the context stream, one after
+    // the other, so each launch's event pair times that kernel alone.
+    cudaStream_t rs = c->prof_on ? c->stream : c->aux;
     for (int t0 = 0; t0 < nz; t0 += kMaxGroup) {  // one table launch per kMaxGroup distances
       const int tn = std::min(kMaxGroup, nz - t0);
       AsmGroupArgs a = group_args(nx, ny, dx, dy, band_limit, evanescent, soft_edge);
@@ -146,7 +149,7 @@ struct SweepPipe {
         if (use_tc) {
           const int nt = gn * (nx / tcfft::kVec);
           LaunchScope ls(c, "tc_sweep_col");
-          tcfft::tc_col_sweep_kernel<<<tc_grid(c, nt, 3), tcfft::kThreads, tcfft::kSmemCol, c->stream>>>(
+          tcfft::tc_col_sweep_kernel<<<tc_grid(c, nt, 2), tcfft::kThreads, tcfft::kSmemBytes, c->stream>>>(
               tcfft::ColSweepTc{spec, w, tab, maxbits, g0}, tcr.F, tcr.tw, nt, tcr.err);
           DOE_CUDA(c, cudaGetLastError());
         } else {
@@ -157,11 +160,11 @@ struct SweepPipe {
           }));
         }
         DOE_CUDA(c, cudaEventRecord(ev_col(g), c->stream));
-        DOE_CUDA(c, cudaStreamWaitEvent(c->aux, ev_col(g), 0));
+        DOE_CUDA(c, cudaStreamWaitEvent(rs, ev_col(g), 0));
         if (use_tc) {
           const int nt = gn * (ny / tcfft::kVec);
-          LaunchScope ls(c, "tc_sweep_row", c->aux);
-          tcfft::tc_row_out_kernel<<<tc_grid(c, nt, 4), tcfft::kThreads, tcfft::kSmemRow, c->aux>>>(
+          LaunchScope ls(c, "tc_sweep_row", rs);
+          tcfft::tc_row_out_kernel<<<tc_grid(c, nt, 2), tcfft::kThreads, tcfft::kSmemBytes, rs>>>(
               tcfft::RowOutTc{w, out_c64 ? out_c64 + o0 : nullptr, out_c64 ? nullptr : out_re + o0,
                               out_c64 ? nullptr : out_im + o0, maxbits, pe},
               tcr.F, tcr.tw, nt, tcr.err);
@@ -169,25 +172,25 @@ struct SweepPipe {
         } else if (out_c64) {
           DOE_TRY(with_row(c, nx, kTuneSweep, [&](auto S) {
             return launch_row<decltype(S)>(c, RowC64<true>{{}, w, out_c64 + o0, nx, ny, pe, pe, 1.f / (float)pe}, gn, ny,
-                                 c->aux);
+                                 rs);
           }));
         } else {
           DOE_TRY(with_row(c, nx, kTuneSweep, [&](auto S) {
             return launch_row<decltype(S)>(
-                c, RowInvToF64{{}, w, out_re + o0, out_im + o0, nx, ny, pe, 1.f / (float)pe}, gn, ny, c->aux);
+                c, RowInvToF64{{}, w, out_re + o0, out_im + o0, nx, ny, pe, 1.f / (float)pe}, gn, ny, rs);
           }));
         }
         for (int i = 0; i < gn; ++i) {
           if (a.z[g0 + i] != 0.0) continue;
           const long o = o0 + (long)i * pe;
           if (out_c64) {
-            DOE_CUDA(c, cudaMemcpyAsync(out_c64 + o, src_c64, pe * sizeof(float2), cudaMemcpyDeviceToDevice, c->aux));
+            DOE_CUDA(c, cudaMemcpyAsync(out_c64 + o, src_c64, pe * sizeof(float2), cudaMemcpyDeviceToDevice, rs));
           } else {
-            DOE_CUDA(c, cudaMemcpyAsync(out_re + o, src_re, pe * sizeof(double), cudaMemcpyDeviceToDevice, c->aux));
-            DOE_CUDA(c, cudaMemcpyAsync(out_im + o, src_im, pe * sizeof(double), cudaMemcpyDeviceToDevice, c->aux));
+            DOE_CUDA(c, cudaMemcpyAsync(out_re + o, src_re, pe * sizeof(double), cudaMemcpyDeviceToDevice, rs));
+            DOE_CUDA(c, cudaMemcpyAsync(out_im + o, src_im, pe * sizeof(double), cudaMemcpyDeviceToDevice, rs));
           }
         }
-        DOE_CUDA(c, cudaEventRecord(ev_row(g), c->aux));
+        DOE_CUDA(c, cudaEventRecord(ev_row(g), rs));
       }
     }
     return DOE_OK;

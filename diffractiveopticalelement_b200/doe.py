@@ -135,11 +135,18 @@ def blurRaster(src, nx, ny, sigmaPx=1.0):
 
 
 # ------------------------------------------------------------------ device loops
+def _nn(d, key, default):
+    """The reference's `d.key ?? default`: the default replaces only a missing or
+    None entry (an explicit 0 or empty value is kept)."""
+    v = d.get(key)
+    return default if v is None else v
+
+
 def _geometry(illumination, o):
-    nx = o.get("nx") or int(round(math.sqrt(len(illumination))))
-    ny = o.get("ny") or nx
-    dx = o.get("dx") or 8e-6
-    dy = o.get("dy") or dx
+    nx = _nn(o, "nx", int(round(math.sqrt(len(illumination)))))
+    ny = _nn(o, "ny", nx)
+    dx = _nn(o, "dx", 8e-6)
+    dy = _nn(o, "dy", dx)
     return int(nx), int(ny), float(dx), float(dy)
 
 
@@ -154,9 +161,8 @@ def _run(algorithm, illumination, targetAmp, o, ctx=None):
     roi = None if o.get("roi") is None else _lib.f64(o["roi"])
     ip = None if o.get("initPhase") is None else _lib.f64(o["initPhase"])
     d = _lib.DesignDesc(nx, ny, dx, dy, float(o["lambda"]), float(o["z"]), algorithm, it,
-                        float(o.get("feedback") or 0.0), int(o.get("escape") or 0),
-                        float(o.get("beta", 0.9) if o.get("beta") is not None else 0.9),
-                        float(o.get("seed", 12345)), _lib.dp(ill), _lib.dp(tgt), _lib.dp(roi), _lib.dp(ip))
+                        float(_nn(o, "feedback", 0.0)), int(_nn(o, "escape", 0)), float(_nn(o, "beta", 0.9)),
+                        float(_nn(o, "seed", 12345)), _lib.dp(ill), _lib.dp(tgt), _lib.dp(roi), _lib.dp(ip))
     res = {"phase": np.empty(n), "amplitude": np.empty(n), "intensity": np.empty(n),
            "error": np.empty(max(it, 1)), "efficiency": np.empty(max(it, 1))}
     wgs = algorithm in (_lib.DOE_ALG_WGS, _lib.DOE_ALG_WGS_FOURIER)
@@ -174,7 +180,7 @@ def _run(algorithm, illumination, targetAmp, o, ctx=None):
         out["weightedIterations"] = it
     cb = o.get("onProgress")
     if cb:
-        every = o.get("progressEvery") or 10
+        every = _nn(o, "progressEvery", 10)
         for i in range(it):
             if i % every == 0 or i == it - 1:
                 cb({"iteration": i, "error": out["error"][i], "efficiency": out["efficiency"][i]})
@@ -254,17 +260,17 @@ def prepareTargetAmp(irradiance, illumination):
 
 def designDOE(cfg, *, ctx=None):
     """Design a projection DOE (src/doe.js:796-896)."""
-    nx = cfg.get("nx") or 256
-    ny = cfg.get("ny") or nx
-    dx = cfg.get("dx") or 8e-6
-    dy = cfg.get("dy") or dx
-    lam = cfg.get("lambda") or 532e-9
-    z = cfg.get("z") if cfg.get("z") is not None else 0.03
-    mode = cfg.get("mode") or "image-plane"
+    nx = _nn(cfg, "nx", 256)
+    ny = _nn(cfg, "ny", nx)
+    dx = _nn(cfg, "dx", 8e-6)
+    dy = _nn(cfg, "dy", dx)
+    lam = _nn(cfg, "lambda", 532e-9)
+    z = _nn(cfg, "z", 0.03)
+    mode = _nn(cfg, "mode", "image-plane")
     alg = cfg.get("algorithm")
-    algorithm = alg if alg and alg != "auto" else ("gs" if mode == "far-field" else "wgs")
-    levels = cfg.get("levels") or 0
-    iterations = cfg.get("iterations") if cfg.get("iterations") is not None else 60
+    algorithm = alg if alg and alg != "auto" else ("gs" if mode == "far-field" else "wgs")  # doe.js:808 (truthy)
+    levels = _nn(cfg, "levels", 0)
+    iterations = _nn(cfg, "iterations", 60)
     illumination = cfg.get("illumination")
     if illumination is None:
         illumination = discMask(nx, ny, dx, dy, (min(nx * dx, ny * dy) / 2) * 0.95, soft=2 * dx)
@@ -272,25 +278,25 @@ def designDOE(cfg, *, ctx=None):
     target = cfg.get("target")
     if target is None:
         target = _default_disc_target(nx, ny, 0.35)
-    if (cfg.get("smooth") or 0) > 0:
+    if _nn(cfg, "smooth", 0) > 0:
         target = blurRaster(target, nx, ny, cfg["smooth"])
     targetAmp = prepareTargetAmp(target, illumination)
     initPhase = cfg.get("initPhase")
     if initPhase is None:
-        init = cfg.get("init") or "random"
+        init = _nn(cfg, "init", "random")
         if init == "flat":
             initPhase = flatPhase(nx, ny)
         elif init == "lens":
             initPhase = kinoformLens(nx, ny, dx, dy, lam, z)
         else:
-            initPhase = randomPhase(nx, ny, cfg.get("seed", 12345))
+            initPhase = randomPhase(nx, ny, _nn(cfg, "seed", 12345))
     common = {
         "nx": nx, "ny": ny, "dx": dx, "dy": dy, "lambda": lam, "z": z, "roi": roi, "iterations": iterations,
-        "seed": cfg.get("seed", 12345),
-        "feedback": (cfg.get("feedback", 0.8) if algorithm == "hio" else 0),
-        "escape": cfg.get("escape") if cfg.get("escape") is not None else int(math.floor(iterations * 0.2 + 0.5)),
-        "beta": cfg.get("beta", 0.9), "initPhase": initPhase, "onProgress": cfg.get("onProgress"),
-        "progressEvery": cfg.get("progressEvery", 10),
+        "seed": _nn(cfg, "seed", 12345),
+        "feedback": (_nn(cfg, "feedback", 0.8) if algorithm == "hio" else 0),
+        "escape": _nn(cfg, "escape", int(math.floor(iterations * 0.2 + 0.5))),
+        "beta": _nn(cfg, "beta", 0.9), "initPhase": initPhase, "onProgress": cfg.get("onProgress"),
+        "progressEvery": _nn(cfg, "progressEvery", 10),
     }
     if mode == "far-field":
         result = (weightedGerchbergSaxton(illumination, targetAmp, common, fourierCgh, ctx=ctx)

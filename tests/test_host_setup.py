@@ -42,3 +42,28 @@ def test_projector_defaults_and_geometry(engine):
     assert P({"n": 128, "mode": "far-field", "distance": 0.02}).z == 0.02
     with pytest.raises(ValueError, match="unknown kind"):
         P({"n": 64, "target": {"kind": "spiral"}})
+
+
+def test_design_doe_defaults_follow_the_reference_nullish_rule(engine, monkeypatch):
+    """designDOE (src/doe.js:796-866) fills a default only where the option is
+    missing or null (`??`): an explicit None takes the default, an explicit 0 is
+    kept. The device loop is intercepted, so this runs without a GPU."""
+    from diffractiveopticalelement_b200 import doe as D
+    seen = {}
+
+    def fake_run(algorithm, illumination, targetAmp, o, ctx=None):
+        seen.update(o)
+        n = int(o["nx"]) * int(o["ny"])
+        return {"phase": np.zeros(n), "error": [], "efficiency": [], "amplitude": np.zeros(n),
+                "intensity": np.zeros(n), "iterations": o["iterations"], "field": None, "rmse": 0.0,
+                "weights": np.ones(n), "weightedIterations": o["iterations"]}
+
+    monkeypatch.setattr(D, "_run", fake_run)
+    r = D.designDOE({"nx": 32, "seed": None, "beta": None, "escape": 0, "iterations": 10, "progressEvery": None,
+                     "z": 0.0})
+    assert seen["seed"] == 12345 and seen["beta"] == 0.9 and seen["progressEvery"] == 10
+    assert seen["escape"] == 0 and seen["z"] == 0.0 and r["z"] == 0.0  # explicit zeros are kept
+    assert np.array_equal(r["illumination"], D.discMask(32, 32, 8e-6, 8e-6, (32 * 8e-6 / 2) * 0.95, soft=16e-6))
+    D.designDOE({"nx": 32, "iterations": 10})
+    assert seen["escape"] == 2  # Math.round(iterations * 0.2)
+    assert np.array_equal(seen["initPhase"], D.randomPhase(32, 32, 12345))
