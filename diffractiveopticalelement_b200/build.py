@@ -46,11 +46,26 @@ def _includes(path: str, seen: set) -> set:
     return seen
 
 
-def _stale(obj: str, src: str) -> bool:
-    if not os.path.exists(obj):
+def _fingerprint(src: str, flags: list[str]) -> str:
+    """SHA-256 of the source, every file it includes and the compile flags."""
+    import hashlib
+    h = hashlib.sha256(" ".join(flags).encode())
+    for path in sorted(_includes(src, set())):
+        h.update(path.encode())
+        with open(path, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def _stale(obj: str, src: str, flags: list[str]) -> bool:
+    """An object is rebuilt unless it exists and was compiled from exactly the
+    current contents of its source and includes (a stamp beside it holds their
+    fingerprint; modification times alone miss an edit made during a build)."""
+    stamp = obj + ".sha256"
+    if not os.path.exists(obj) or not os.path.exists(stamp):
         return True
-    t = os.path.getmtime(obj)
-    return any(os.path.getmtime(d) > t for d in _includes(src, set()))
+    with open(stamp) as f:
+        return f.read().strip() != _fingerprint(src, flags)
 
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
@@ -60,19 +75,25 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
 
     def compile_one(src):
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
-        if _stale(obj, src) or extra:
-            cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+        flags = [*ARCH, *FLAGS, *extra]
+        if _stale(obj, src, flags):
+            fp = _fingerprint(src, flags)  # taken before compiling: a later edit leaves the object stale
+            cmd = [nvcc, *flags, "-c", src, "-o", obj]
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
             if verbose and r.stderr:
                 sys.stderr.write(r.stderr)
-        return obj
+            with open(obj + ".sha256", "w") as f:
+                f.write(fp)
+            return obj, True
+        return obj, False
 
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(compile_one, sources()))
+        done = list(ex.map(compile_one, sources()))
+    objs = [o for o, _ in done]
     newest = max(os.path.getmtime(o) for o in objs)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+    if any(r for _, r in done) or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

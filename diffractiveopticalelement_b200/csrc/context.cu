@@ -76,7 +76,8 @@ extern "C" int doe_ctx_synchronize(doe_ctx* c) {
   if (!c) return DOE_ERR_BAD_ARG;
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   DOE_CUDA(c, cudaStreamSynchronize(c->aux));
-  return tc_check(c);  // a timed-out wait of an asynchronous tensor-core pass surfaces here
+  DOE_TRY(tc_check(c));  // a timed-out wait of an asynchronous tensor-core pass surfaces here
+  return design_error_check(c);  // ... and one of the cluster-resident design loop
 }
 
 extern "C" unsigned long long doe_ctx_launch_count(doe_ctx* c) { return c ? c->launches : 0ull; }
@@ -133,6 +134,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_graph;
   } else if (k == "sweep_tc") {
     *value = c->tune_sweep_tc;
+  } else if (k == "design_cluster") {
+    *value = c->tune_design_cluster;
   } else {
     return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
   }
@@ -152,6 +155,10 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   }
   if (k == "sweep_tc") {
     c->tune_sweep_tc = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "design_cluster") {
+    c->tune_design_cluster = value ? 1 : 0;
     return DOE_OK;
   }
   if (k == "sweep_group") {

@@ -422,6 +422,7 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   DOE_CUDA(c, cudaMemcpyAsync(hout.data(), o, hout.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   DOE_CUDA(c, cudaMemcpyAsync(hh.data(), hist, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+  DOE_TRY(design_error_check(c));
   for (int i = 0; i < nb; ++i) {
     memcpy(r[i].phase, hout.data() + i * n, n * sizeof(double));
     const double* am = hout.data() + Bn + i * n;

@@ -657,23 +657,13 @@ struct RowPhaseGrad : NoReduce {
   }
 };
 
-// Design loops are compiled for power-of-two axes 32..4096 with the default CTA
-// shapes (each operator is instantiated once per size).
-constexpr int kDesignMinN = 32, kDesignMaxN = 4096;
+// Design loops are compiled for every power-of-two axis the transforms take,
+// 1..8192, with the default CTA shapes (each operator is instantiated once per size).
+constexpr int kDesignMinN = 1, kDesignMaxN = kMaxN;
 
 template <class F>
 inline int with_design_n(int n, F&& f) {
-  switch (n) {
-    case 32: return f(std::integral_constant<int, 32>{});
-    case 64: return f(std::integral_constant<int, 64>{});
-    case 128: return f(std::integral_constant<int, 128>{});
-    case 256: return f(std::integral_constant<int, 256>{});
-    case 512: return f(std::integral_constant<int, 512>{});
-    case 1024: return f(std::integral_constant<int, 1024>{});
-    case 2048: return f(std::integral_constant<int, 2048>{});
-    case 4096: return f(std::integral_constant<int, 4096>{});
-    default: return DOE_ERR_UNSUPPORTED;
-  }
+  return with_n(n, static_cast<F&&>(f));
 }
 template <class Op>
 inline int design_row(doe_ctx* c, const Op& op, int B, int nx, int ny) {
@@ -706,6 +696,9 @@ inline int design_bpp(int nx, int ny) {
 // design_fourier.cu); the state in `b` is initialised by the caller.
 int design_run_gs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
 int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int iterations);
+// Image-plane WGS with the whole loop resident in one thread-block cluster per
+// design (square 64^2, 128^2, 256^2); DOE_ERR_UNSUPPORTED for other grids.
+int design_run_wgs_cluster(doe_ctx* c, const DesignBufs& b, int B, int iterations);
 int design_run_fourier(doe_ctx* c, const DesignBufs& b, int B, int iterations, bool wgs);
 // Multi-plane (B designs): plane p uses transfer table htab + p*n and target /
 // ROI planes tgt0 + d*nplanes*n + p*n (roi0 may be null).

@@ -5,6 +5,10 @@
 namespace doe {
 
 int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int I) {
+  if (c->tune_design_cluster) {  // 64^2, 128^2, 256^2: the whole loop in one cluster per design
+    const int rc = design_run_wgs_cluster(c, b, B, I);
+    if (rc != DOE_ERR_UNSUPPORTED) return rc;
+  }
   const int nx = b.nx, ny = b.ny;
   const float scale = 1.f / (float)((long)nx * ny);
   const ColAsmTab<false> fwd{{}, b.W, b.htab, b.htab_stride, nx, ny, b.st};

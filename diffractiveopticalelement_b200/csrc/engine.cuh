@@ -32,6 +32,7 @@ enum Slot {
   kSlotDesign2,
   kSlotTc,       // tensor-core FFT tables and error flag
   kSlotTcMax,    // per-field spectrum maxima (tensor-core input scale)
+  kSlotErr,      // error word of the cluster-resident design loop
   kSlotCount
 };
 
@@ -53,6 +54,7 @@ struct doe_ctx {
   unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
   int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
+  int tune_design_cluster = 0;         // 1: 64^2-256^2 image-plane WGS runs cluster-resident
   void* tc_tables = nullptr;           // tensor-core tables built in this slot allocation
   int num_sms = 0;
   unsigned long long slot_gen = 0;     // bumped whenever a scratch slot is reallocated
@@ -100,6 +102,13 @@ inline bool is_pow2(long n) { return n > 0 && (n & (n - 1)) == 0; }
 // Reads and clears the device error flag of the tensor-core passes (prop_sweep.cu);
 // the context's streams must be synchronised.
 int tc_check(doe_ctx* c);
+
+// Error word of the cluster-resident design loop (design_cluster.cu): a kernel whose
+// bounded cluster-barrier wait ran out stores a nonzero code there. design_error_word
+// gives its address (allocated and zeroed on first use, outside any capture);
+// design_error_check reads and clears it once the context's streams are synchronised.
+int design_error_word(doe_ctx* c, int** out);
+int design_error_check(doe_ctx* c);
 
 inline int check_grid(doe_ctx* c, int nx, int ny, const char* who) {
   if (!is_pow2(nx) || !is_pow2(ny))

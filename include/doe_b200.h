@@ -75,11 +75,16 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * element in the sweep column pass (0: all reads first); "sweep_graph" = 0 to
  * disable CUDA-graph replay of repeated device sweeps; "sweep_tc" = 0 to run
  * 1024 x 1024 focus sweeps on the FP32 CUDA-core passes instead of the tcgen05
- * tensor-core passes (default 1); "fft_row", "fft_col",
+ * tensor-core passes (default 1); "design_cluster" = 1 to run image-plane
+ * weightedGerchbergSaxton on square 64^2, 128^2 and 256^2 grids as one
+ * on-chip loop per design (a thread-block cluster holding the plane in
+ * distributed shared memory) instead of five passes per iteration (default 0);
+ * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
-/* Current value of "sweep_group", "sweep_fused", "sweep_graph" or "sweep_tc". */
+/* Current value of "sweep_group", "sweep_fused", "sweep_graph", "sweep_tc" or
+ * "design_cluster". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for

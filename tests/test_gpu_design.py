@@ -211,10 +211,28 @@ def test_design_is_deterministic_and_batch_equals_single(engine):
 
 def test_design_rejects_unsupported_grids(engine):
     from diffractiveopticalelement_b200 import DOEError
-    with pytest.raises(DOEError, match="design grids"):
-        engine.gerchbergSaxton(np.ones(16 * 16), np.ones(16 * 16), {"nx": 16, "iterations": 2})
+    with pytest.raises(DOEError, match="power-of-two"):
+        engine.gerchbergSaxton(np.ones(24 * 24), np.ones(24 * 24), {"nx": 24, "ny": 24, "iterations": 2})
     with pytest.raises(ValueError, match="no planes"):
         engine.gerchbergSaxtonMultiPlane(np.ones(64 * 64), [], {"nx": 64})
+
+
+@pytest.mark.parametrize("nx,ny", [(1, 1), (2, 2), (8, 8), (16, 16), (16, 8), (8192, 16), (16, 8192)])
+@pytest.mark.parametrize("alg", ["gs", "wgs", "fourier"])
+def test_design_grids_across_the_whole_power_of_two_range(engine, oracle, nx, ny, alg):
+    """The reference designs on any power-of-two grid (src/field.js:30-32): the
+    smallest grids and 8192-point axes run here too, with field parity."""
+    n = nx * ny
+    rng = np.random.default_rng(7 * nx + ny)
+    ill = 0.5 + 0.5 * rng.uniform(0, 1, n)
+    tgt = rng.uniform(0.1, 1, n)
+    ip = rng.uniform(-np.pi, np.pi, n)
+    opts = {"nx": nx, "ny": ny, "dx": DX, "lambda": LAMBDA, "z": 0.03, "iterations": 2, "initPhase": ip}
+    fn = {"gs": engine.gerchbergSaxton, "wgs": engine.weightedGerchbergSaxton, "fourier": engine.fourierCgh}[alg]
+    g = fn(ill, tgt, opts)
+    o = oracle.design(alg, ill, tgt, nx=nx, ny=ny, dx=DX, lam=LAMBDA, z=0.03, iterations=2, init_phase=ip)
+    assert rel_l2(doe_field(ill, np.asarray(g["phase"])), doe_field(ill, o["phase"])) < TOL
+    assert rel_l2(g["amplitude"], o["amplitude"]) < TOL
 
 
 # ------------------------------------------------------------------ screen-RMSE stopping goal

@@ -51,15 +51,22 @@ def test_forward_and_gradients_match_oracle(engine, n, base, levels, B):
     # BF16 activations: a value whose FP32 sum lands on the other side of a BF16
     # rounding boundary than the oracle's FP64 sum differs by one BF16 ulp, and the
     # deep chain spreads that; the bounds below sit well inside what a wrong
-    # transpose, flip, mask or scale produces (cosine near 0 or a ratio far from 1)
+    # transpose, flip, mask or scale produces (cosine near 0 or a ratio far from 1).
+    # The least-squares scale a = <g, g_o> / |g_o|^2 is what a wrong factor moves
+    # (1.2 for a 20 % error) while rounding noise, uncorrelated with g_o, leaves it
+    # near 1 (measured on B200: 0.95-1.00 overall, 0.98-1.013 per layer): it is
+    # held to 10 % overall and per layer.
     cos = lambda x, y: float(x @ y / (np.linalg.norm(x) * np.linalg.norm(y) + 1e-300))
-    print("overall rel", rel_l2(g, g_o), "cos", cos(g, g_o))
+    fit = lambda x, y: float(x @ y / (y @ y + 1e-300))
+    print("overall rel", rel_l2(g, g_o), "cos", cos(g, g_o), "scale", fit(g, g_o))
     assert rel_l2(g, g_o) < 0.2 and cos(g, g_o) > 0.99
+    assert abs(fit(g, g_o) - 1) < 0.1
     o = 0
     for ci, co in U.layer_shapes(base, levels):  # per layer, so no layer hides behind the others
         k = co * 9 * ci
-        print((ci, co), rel_l2(g[o:o + k], g_o[o:o + k]), cos(g[o:o + k], g_o[o:o + k]))
-        assert rel_l2(g[o:o + k], g_o[o:o + k]) < 0.3 and cos(g[o:o + k], g_o[o:o + k]) > 0.97, (ci, co)
+        w, wo = g[o:o + k], g_o[o:o + k]
+        print((ci, co), rel_l2(w, wo), cos(w, wo), fit(w, wo))
+        assert rel_l2(w, wo) < 0.3 and cos(w, wo) > 0.97 and abs(fit(w, wo) - 1) < 0.1, (ci, co)
         assert rel_l2(g[o + k:o + k + co], g_o[o + k:o + k + co]) < 0.3, (ci, co, "bias")
         o += k + co
     assert rel_l2(g[o:], g_o[o:]) < 2e-2  # head
