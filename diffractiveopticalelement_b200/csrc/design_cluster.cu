@@ -36,17 +36,19 @@ namespace {
 
 constexpr uint64_t kClusterWaitNs = 1000000000ull;
 
+// 512 threads (16 warps) per CTA and one CTA per SM: a batch of a row pass
+// transforms 512 / T rows, one of a column pass 512 / T columns (T threads per
+// transform, the default plan of length N).
 template <int N>
 struct ClusterGeom {
   static constexpr int R = N >= 256 ? 4 : 1;  // CTAs per design
   static constexpr int ROWS = N / R;          // rows per CTA
-  using RS = typename DefRow<N>::type;
-  using CS = typename DefCol<N>::type;
-  using P = typename RS::Plan;
-  static_assert(std::is_same<P, typename CS::Plan>::value, "row and column passes share the plan");
-  static_assert(RS::THREADS == 256 && CS::THREADS == 256, "one 256-thread CTA shape for both passes");
+  static constexpr int THREADS = 512;
+  using P = typename DefaultPlan<N>::type;
+  using RS = RowShape<P, THREADS / P::T>;
+  using CS = ColShape<P, THREADS / P::T>;
+  static_assert(RS::THREADS == THREADS && CS::THREADS == THREADS, "one CTA shape for both passes");
   static_assert(ROWS % RS::V == 0 && ROWS % CS::C == 0, "batches tile the CTA's rows and columns");
-  static constexpr int THREADS = 256;
   static constexpr int SCRATCH = RS::SMEM > CS::SMEM ? RS::SMEM : CS::SMEM;
   static constexpr int PLANE_BYTES = ROWS * N * 8;
   static constexpr int RED_OFF = PLANE_BYTES + SCRATCH;  // [R][kRedKGoal] doubles, 8-byte aligned
@@ -133,6 +135,10 @@ struct ClusterWgs {
   // Row pass over this CTA's rows: `load(y, x)` gives the input, `mid(y, x, v)`
   // acts between the two transforms (when STAGES == 2), `store(y, x, v, acc)`
   // consumes the output. All threads of the CTA take part (batches of V rows).
+  // The side planes are read where they are used: an L1 prefetch of a whole
+  // batch's lines ahead of the transform (as the multi-pass kernels do) measured
+  // ~8 % slower here, the 32-row batch's lines exceeding what is left of L1 next
+  // to the shared memory, and the extra load instructions throttling the LSU.
   template <bool INV1, bool INV2, int STAGES, class Load, class Mid, class Store>
   __device__ __forceinline__ void row_pass(const Plane& pl, float2* scratch, int row0, Load load, Mid mid,
                                            Store store, DAcc<K>& acc) const {
@@ -168,6 +174,8 @@ struct ClusterWgs {
 #pragma unroll 1
     for (int b0 = 0; b0 < G::ROWS; b0 += C) {
       const int x = col0 + b0 + c;
+#pragma unroll
+      for (int q = 0; q < RMAX; ++q) prefetch_l1(&htab[(long)out_elem<P>(t, q) * N + x]);
       float2 v[RMAX];
 #pragma unroll
       for (int q = 0; q < RMAX; ++q) v[q] = *pl.at(in_elem<P>(t, q), x);
@@ -433,7 +441,7 @@ struct ClusterWgs {
 };
 
 template <int N, bool GOAL>
-__global__ void __launch_bounds__(256, 1) wgs_cluster_kernel(ClusterWgs<N, GOAL> k) {
+__global__ void __launch_bounds__(512, 1) wgs_cluster_kernel(ClusterWgs<N, GOAL> k) {
   k.run();
 }
 
