@@ -193,6 +193,9 @@ PASS_BYTES_PX = {
     "design_row_doe_fwd": 16,                                 # A, phase in, W out
     "design_col_fourier": 28, "design_col_fourier_wgs": 36,   # W in/out, t, m in, amplitude out (+ w in/out)
     "design_row_gs_target": 24, "design_row_gs_final": 20,    # W in/out, t, m in (final: amplitude out)
+    # the cluster-resident WGS loop, one launch for the fixed 100 iterations: only the
+    # side planes move (t, m, w in + w out twice, A in, phase out, the table twice)
+    "design_wgs_cluster": 52 * 100,
 }
 
 
@@ -221,6 +224,19 @@ WGS_CONFIG = {"workload": "wgs256", "grid": [256, 256], "max_iterations": 100,
               "targets": "3-8 seeded rectangles 4-40 px in the central 128^2, autoRoi", "band_limit": False}
 
 
+def tune_wgs(ctx, n_designs, rank=0, trial_iterations=4):
+    """Design-pass autotuning (doe_autotune_design) on this rank's own C1 batch,
+    before any timing: shape variants of the passes and the cluster-resident loop."""
+    import torch
+    from diffractiveopticalelement_b200 import batch
+    ill, irr, roi, tgt, ph = wgs_inputs(n_designs, seed0=1 + rank * n_designs)
+    f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+    ch = batch.autotune_design(ctx, f32(ill), f32(tgt), f32(ph), nx=WGS_N, ny=WGS_N, dx=WGS_DX, lam=WGS_LAM,
+                               z=WGS_Z, iterations=WGS_ITERS, roi=f32(roi), trial_iterations=trial_iterations)
+    return {"row_variant": ch[0], "col_variant": ch[1], "cluster_loop": ch[2], "trial_iterations": trial_iterations,
+            "tuner": "doe_autotune_design (fastest of every pass shape variant and the cluster loop, timed)"}
+
+
 def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=0, world=1):
     """C1 (plain GPU WGS to the goal) and C4 (surrogate warm start + WGS to the goal)
     on the same seeded designs, the fixed 100-iteration loop (all designs active,
@@ -228,6 +244,7 @@ def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=
     on one."""
     import torch
     import torch.distributed as dist
+    tuning = tune_wgs(ctx, designs, rank)
     r = run_wgs(ctx, device, designs, max(warmup, 3), steps, goal=0.01, rank=rank)
     fixed = run_wgs(ctx, device, designs, 1, 1, rank=rank)
     ms, reached = r["ms_per_step"], r["reached"]
@@ -243,7 +260,7 @@ def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=
         roof["basis"] = ("dominant pass of the fixed 100-iteration loop (every design active): bytes per pixel x "
                          "designs x 256^2 over its average launch time")
     out = {"metric": WGS_METRIC, "value": reached / (ms / 1e3), "unit": "designs/s", "ms_per_step": ms,
-           "config": dict(WGS_CONFIG, designs=designs), "roofline": roof, "wgs256": r,
+           "config": dict(WGS_CONFIG, designs=designs, design_tuning=tuning), "roofline": roof, "wgs256": r,
            "fixed_100_iterations": fixed, "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
     if surrogate_steps > 0:
         warm = run_warm(ctx, device, designs, surrogate_steps)

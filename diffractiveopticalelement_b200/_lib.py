@@ -120,6 +120,7 @@ def _declare(L):
                                        _vp]),
         "doe_design_batch": (i, [ctxp, i, C.POINTER(DesignDesc), C.POINTER(DesignResult)]),
         "doe_design_dev": (i, [ctxp, C.POINTER(DesignDevDesc)]),
+        "doe_autotune_design": (i, [ctxp, C.POINTER(DesignDevDesc), i, C.POINTER(C.c_int)]),
         "doe_multiplane_dev": (i, [ctxp, C.POINTER(MultiplaneDevDesc)]),
         "doe_phase_loss_grad": (i, [ctxp, C.POINTER(PhaseLossDesc)]),
         "doe_design_multi_create": (i, [ctxp, C.POINTER(C.c_void_p)]),

@@ -67,6 +67,34 @@ def design_batch(ctx, illumination, target_amp, phase, *, nx, ny, dx, dy=None, l
     WGS) a design stops at the first iteration whose screen RMSE is <= rmse_goal
     and `iterations_used` says when. Returns a dict of device tensors.
     """
+    desc, out = _design_desc(illumination, target_amp, phase, nx=nx, ny=ny, dx=dx, dy=dy, lam=lam, z=z,
+                             iterations=iterations, algorithm=algorithm, beta=beta, feedback=feedback, escape=escape,
+                             roi=roi, lambdas=lambdas, zs=zs, rmse_goal=rmse_goal, screen_irr=screen_irr,
+                             history=history)
+    with _Ordered(ctx):
+        ctx.check(ctx.lib.doe_design_dev(ctx.h, C.byref(desc)))
+    return out
+
+
+def autotune_design(ctx, illumination, target_amp, phase, *, trial_iterations=4, **kw):
+    """Pick the fastest design-pass shapes (and, for image-plane WGS on 64^2-256^2,
+    the cluster-resident loop) for this batch's grid (doe_autotune_design).
+
+    Takes design_batch's arguments; runs `trial_iterations` iterations per
+    candidate, leaves `phase` as it was and keeps the choice in the context.
+    Returns (row variant, column variant, cluster loop)."""
+    desc, _ = _design_desc(illumination, target_amp, phase, **kw)
+    chosen = (C.c_int * 3)()
+    with _Ordered(ctx):
+        ctx.check(ctx.lib.doe_autotune_design(ctx.h, C.byref(desc), int(trial_iterations), chosen))
+    return tuple(chosen)
+
+
+def _design_desc(illumination, target_amp, phase, *, nx, ny, dx, dy=None, lam=532e-9, z=0.03, iterations=100,
+                 algorithm="wgs", beta=0.9, feedback=0.0, escape=0, roi=None, lambdas=None, zs=None, rmse_goal=0.0,
+                 screen_irr=None, history=True):
+    """The doe_design_dev descriptor of a batch and the dict of its output tensors
+    (the descriptor's host arrays are kept alive in the dict)."""
     torch = _torch()
     if algorithm not in _ALG:
         raise ValueError(f"unknown algorithm {algorithm!r}")
@@ -97,14 +125,13 @@ def design_batch(ctx, illumination, target_amp, phase, *, nx, ny, dx, dy=None, l
                               _ALG[algorithm], int(iterations), float(feedback), int(escape), float(beta),
                               ptr(ill), ptr(tgt), ptr(ro), ptr(ph), ptr(amp), None, ptr(err), ptr(eff), ptr(rmse),
                               float(rmse_goal), ptr(sirr), ptr(used) if algorithm == "wgs" else None)
-    with _Ordered(ctx):
-        ctx.check(ctx.lib.doe_design_dev(ctx.h, C.byref(desc)))
     out = {"phase": ph, "amplitude": amp, "error": err, "efficiency": eff}
     if wgs:
         out["rmse"] = rmse
     if algorithm == "wgs":
         out["iterations_used"] = used
-    return out
+    desc._keep = (ill, tgt, ro, sirr, lam_a, z_a)  # inputs the descriptor points into
+    return desc, out
 
 
 def screen_metrics_batch(ctx, amplitude, target_irr, illumination, *, nx, ny, sdx, sdy=None, dx=None, dy=None,

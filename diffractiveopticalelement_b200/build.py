@@ -94,7 +94,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     objs = [o for o, _ in done]
     newest = max(os.path.getmtime(o) for o in objs)
     if any(r for _, r in done) or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [nvcc, *ARCH, "-shared", "-Xlinker", "-z,defs", "-o", LIB, *objs, "-lcudart"]  # no unresolved symbols
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -135,7 +135,7 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
   } else if (k == "sweep_tc") {
     *value = c->tune_sweep_tc;
   } else if (k == "design_cluster") {
-    *value = c->tune_design_cluster;
+    *value = (long long)c->tune_design_cluster;  // bit log2(n) set: n^2 runs cluster-resident
   } else {
     return set_err(c, DOE_ERR_BAD_ARG, "unknown tuning key '%s'", key);
   }
@@ -158,7 +158,16 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
     return DOE_OK;
   }
   if (k == "design_cluster") {
-    c->tune_design_cluster = value ? 1 : 0;
+    // 0 / 1: every size it covers (64^2, 128^2, 256^2) off / on;
+    // (log2(n) << 8) | on: that size alone
+    if (value >= 256) {
+      const int lg = (int)((value >> 8) & 0xff);
+      if (lg > kMaxLog2) return set_err(c, DOE_ERR_BAD_ARG, "tuning: log2 length %d out of range", lg);
+      const unsigned bit = 1u << lg;
+      c->tune_design_cluster = (value & 1) ? (c->tune_design_cluster | bit) : (c->tune_design_cluster & ~bit);
+    } else {
+      c->tune_design_cluster = value ? ((1u << 6) | (1u << 7) | (1u << 8)) : 0u;
+    }
     return DOE_OK;
   }
   if (k == "sweep_group") {

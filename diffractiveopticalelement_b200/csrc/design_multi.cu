@@ -46,6 +46,10 @@ int submit(doe_design_multi* m, int k, const doe_design_dev_desc* d, unsigned lo
   for (int i = 0; i < k; ++i) n0 += m->sub[i]->launches;
   for (int i = 0; i < k; ++i) {
     doe_ctx* s = m->sub[i];
+    // the classes run with the parent's design tuning (shape variants, cluster loop)
+    memcpy(s->tune_row[kTuneDesign], c->tune_row[kTuneDesign], sizeof(c->tune_row[kTuneDesign]));
+    memcpy(s->tune_col[kTuneDesign], c->tune_col[kTuneDesign], sizeof(c->tune_col[kTuneDesign]));
+    s->tune_design_cluster = c->tune_design_cluster;
     DOE_CUDA(c, cudaStreamWaitEvent(s->stream, m->fork, 0));
     const int rc = doe_design_dev(s, &d[i]);
     if (rc) return set_err(c, rc, "design multi: class %d: %s", i, s->err.c_str());

@@ -665,31 +665,72 @@ template <class F>
 inline int with_design_n(int n, F&& f) {
   return with_n(n, static_cast<F&&>(f));
 }
+// Row / column pass of a design loop with the shape variant the context selected
+// for that length (tuning kind "design"; doe_autotune_design picks it). Each
+// operator's passes, for every length and shape variant, are instantiated once,
+// in one of the design_inst_*.cu units (which define DOE_DESIGN_INSTANTIATE), so
+// that those heavy kernel instantiations compile in parallel; the pass sequences
+// only see the declarations.
 template <class Op>
-inline int design_row(doe_ctx* c, const Op& op, int B, int nx, int ny) {
+int design_row(doe_ctx* c, const Op& op, int B, int nx, int ny);
+template <class Op>
+int design_col(doe_ctx* c, const Op& op, int B, int nx, int ny);
+
+#ifdef DOE_DESIGN_INSTANTIATE
+template <class Op>
+int design_row(doe_ctx* c, const Op& op, int B, int nx, int ny) {
   return with_design_n(nx, [&](auto NC) {
-    return launch_row<typename DefRow<decltype(NC)::value>::type>(c, op, B, ny);
+    constexpr int N = decltype(NC)::value;
+    auto f = [&](auto S) { return launch_row<decltype(S)>(c, op, B, ny); };
+    return select_shape<typename DesignRowVariants<N>::list>(c->tune_row[kTuneDesign][ilog2i(N)], f);
   });
 }
 template <class Op>
-inline int design_col(doe_ctx* c, const Op& op, int B, int nx, int ny) {
+int design_col(doe_ctx* c, const Op& op, int B, int nx, int ny) {
   return with_design_n(ny, [&](auto NC) {
-    return launch_col<typename DefCol<decltype(NC)::value>::type>(c, op, B, nx);
+    constexpr int N = decltype(NC)::value;
+    auto f = [&](auto S) { return launch_col<decltype(S)>(c, op, B, nx); };
+    return select_shape<typename DesignColVariants<N>::list>(c->tune_col[kTuneDesign][ilog2i(N)], f);
   });
 }
+#define DOE_DESIGN_ROW_INST(...) template int design_row<__VA_ARGS__>(doe_ctx*, const __VA_ARGS__&, int, int, int);
+#define DOE_DESIGN_COL_INST(...) template int design_col<__VA_ARGS__>(doe_ctx*, const __VA_ARGS__&, int, int, int);
+#endif
+
+// CTAs per design of the widest pass over every shape variant (sizes the
+// per-block reduction partials whatever variant a later call selects).
 inline int design_bpp(int nx, int ny) {
   int bpp = 1;
   with_design_n(nx, [&](auto NC) {
-    using S = typename DefRow<decltype(NC)::value>::type;
-    bpp = std::max(bpp, (ny + S::V - 1) / S::V);
+    auto f = [&](auto S) {
+      bpp = std::max(bpp, (ny + decltype(S)::V - 1) / decltype(S)::V);
+      return 0;
+    };
+    using L = typename DesignRowVariants<decltype(NC)::value>::list;
+    for (int v = 0; v < (int)std::tuple_size<L>::value; ++v) select_shape<L>(v, f);
     return 0;
   });
   with_design_n(ny, [&](auto NC) {
-    using S = typename DefCol<decltype(NC)::value>::type;
-    bpp = std::max(bpp, (nx + S::C - 1) / S::C);
+    auto f = [&](auto S) {
+      bpp = std::max(bpp, (nx + decltype(S)::C - 1) / decltype(S)::C);
+      return 0;
+    };
+    using L = typename DesignColVariants<decltype(NC)::value>::list;
+    for (int v = 0; v < (int)std::tuple_size<L>::value; ++v) select_shape<L>(v, f);
     return 0;
   });
   return bpp;
+}
+// Number of design-pass shape variants for length n (for the autotuner).
+inline int design_row_variants(int n) {
+  return with_design_n(n, [](auto NC) {
+    return (int)std::tuple_size<typename DesignRowVariants<decltype(NC)::value>::list>::value;
+  });
+}
+inline int design_col_variants(int n) {
+  return with_design_n(n, [](auto NC) {
+    return (int)std::tuple_size<typename DesignColVariants<decltype(NC)::value>::list>::value;
+  });
 }
 
 // Pass sequences, one translation unit each (design_gs.cu, design_wgs.cu,

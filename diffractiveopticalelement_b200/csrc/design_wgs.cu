@@ -5,7 +5,8 @@
 namespace doe {
 
 int design_run_wgs(doe_ctx* c, const DesignBufs& b, int B, int I) {
-  if (c->tune_design_cluster) {  // 64^2, 128^2, 256^2: the whole loop in one cluster per design
+  // 64^2, 128^2, 256^2 (when selected): the whole loop in one cluster per design
+  if (b.nx == b.ny && ((c->tune_design_cluster >> ilog2i(b.nx)) & 1u)) {
     const int rc = design_run_wgs_cluster(c, b, B, I);
     if (rc != DOE_ERR_UNSUPPORTED) return rc;
   }

@@ -54,7 +54,7 @@ struct doe_ctx {
   unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
   int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
-  int tune_design_cluster = 0;         // 1: 64^2-256^2 image-plane WGS runs cluster-resident
+  unsigned tune_design_cluster = 0;    // bit log2(n): square n^2 image-plane WGS runs cluster-resident
   void* tc_tables = nullptr;           // tensor-core tables built in this slot allocation
   int num_sms = 0;
   unsigned long long slot_gen = 0;     // bumped whenever a scratch slot is reallocated

@@ -122,6 +122,30 @@ struct ColVariants<2048> {
   using list = std::tuple<ColShape<FftPlan<2048, 3, 16, 8, 16>, 4>, ColShape<FftPlan<2048, 3, 32, 2, 32>, 4>,
                           ColShape<FftPlan<2048, 3, 16, 8, 16>, 2>, ColShape<FftPlan<2048, 3, 32, 2, 32>, 8>>;
 };
+// Shape variants of the design-loop passes: the default plan of length N in every
+// variant (so a variant changes how lines are grouped into CTAs and the register
+// cap, never the transform's arithmetic), for the lengths the benchmarked design
+// loops use. Index 0 is the default; 1 toggles the register cap between one and
+// two resident CTAs; 2 halves the lines per CTA with a cap for four CTAs per SM.
+template <int N>
+struct DesignRowVariants {
+  using D = typename DefRow<N>::type;
+  using P = typename D::Plan;
+  using list = std::conditional_t<
+      (N >= 64 && N <= 2048),
+      std::tuple<D, RowShape<P, D::V, (D::MINB == 2 ? 1 : 2)>, RowShape<P, (D::V > 1 ? D::V / 2 : 1), 4>>,
+      std::tuple<D>>;
+};
+template <int N>
+struct DesignColVariants {
+  using D = typename DefCol<N>::type;
+  using P = typename D::Plan;
+  using list = std::conditional_t<
+      (N >= 64 && N <= 2048),
+      std::tuple<D, ColShape<P, D::C, (D::MINB == 2 ? 1 : 2)>, ColShape<P, (D::C > 2 ? D::C / 2 : 1), 4>>,
+      std::tuple<D>>;
+};
+
 template <>
 struct RowVariants<512> {
   using list = std::tuple<RowShape<FftPlan<512, 3, 8, 8, 8>, 4>, RowShape<FftPlan<512, 2, 16, 32>, 16>,

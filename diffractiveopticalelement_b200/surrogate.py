@@ -37,9 +37,12 @@ class Surrogate:
         self.count = int(self.ctx.lib.doe_surrogate_param_count(h))
 
     def close(self):
-        if self.h:
+        # the network's memory is released through its context; once that context
+        # is gone (interpreter shutdown collects the two in any order) the process
+        # is ending and the driver releases everything
+        if self.h and getattr(self.ctx, "h", None):
             self.ctx.lib.doe_surrogate_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

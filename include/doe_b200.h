@@ -78,7 +78,9 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * tensor-core passes (default 1); "design_cluster" = 1 to run image-plane
  * weightedGerchbergSaxton on square 64^2, 128^2 and 256^2 grids as one
  * on-chip loop per design (a thread-block cluster holding the plane in
- * distributed shared memory) instead of five passes per iteration (default 0);
+ * distributed shared memory) instead of five passes per iteration, 0 for the
+ * passes on all three (default), or (log2(n) << 8) | on for one grid size;
+ * its current value reads back as a mask with bit log2(n) set per size on;
  * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
@@ -275,6 +277,20 @@ typedef struct doe_design_dev_desc {
   int* iterations_used;
 } doe_design_dev_desc;
 int doe_design_dev(doe_ctx* ctx, const doe_design_dev_desc* desc);
+
+/* Autotuner of the design loops (engine-only; no reference counterpart): runs
+ * the design described by desc for `iterations` iterations (<= 0: 4; the
+ * screen-RMSE goal is ignored) with every shape variant of its row and column
+ * passes -- the same FFT plan in every variant, so the arithmetic of a pass does
+ * not change, only how its lines are grouped into CTAs and its register cap --
+ * and, for image-plane WGS on a square 64^2, 128^2 or 256^2 grid, with the
+ * cluster-resident loop; keeps the fastest in the context ("design_row" /
+ * "design_col" variants for those lengths, the grid's "design_cluster" entry).
+ * desc's output arrays are scratch during the trials; desc->phase is restored to
+ * the initial phase. Allocates one phase-sized buffer for the duration of the
+ * call and synchronises the stream. chosen (3 ints, may be NULL) receives {row
+ * variant, column variant, cluster loop 0/1}. */
+int doe_autotune_design(doe_ctx* ctx, const doe_design_dev_desc* desc, int iterations, int* chosen);
 
 /* Designs of uneven sizes in one submission (no reference counterpart): each
  * descriptor is one size class (B designs of one grid) and runs on its own
