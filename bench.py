@@ -967,10 +967,13 @@ def main():
         ctx.check(L.doe_autotune(ctx.h, NX, NY, DX, DX, 532e-9, 0.03, chosen))
     fused = C.c_longlong(0)
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_fused", C.byref(fused)))
-    graph = C.c_longlong(0)
+    graph, hsym, tc = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_graph", C.byref(graph)))
+    ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_hsym", C.byref(hsym)))
+    ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_tc", C.byref(tc)))
     tuned = {"fft_row": chosen[0], "fft_col": chosen[1], "sweep_row": chosen[2], "sweep_col": chosen[3],
-             "sweep_group": chosen[4], "sweep_fused_load": int(fused.value), "sweep_graph": int(graph.value)}
+             "sweep_group": chosen[4], "sweep_fused_load": int(fused.value), "sweep_mirror_h": int(hsym.value),
+             "sweep_tensor_core": int(tc.value), "sweep_graph": int(graph.value)}
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         step()

@@ -53,6 +53,7 @@ struct doe_ctx {
   cudaGraphExec_t sweep_exec = nullptr;  // graph of the last repeated device sweep
   unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
+  int tune_sweep_hsym = 0;             // 1: sweep column pass shares H between mirrored rows
   int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
   unsigned tune_design_cluster = 0;    // bit log2(n): square n^2 image-plane WGS runs cluster-resident
   void* tc_tables = nullptr;           // tensor-core tables built in this slot allocation

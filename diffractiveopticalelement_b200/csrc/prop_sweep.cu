@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "ops_propagate.cuh"
+#include "sweep_sym.cuh"
 #include "tc_fft.cuh"
 
 using namespace doe;
@@ -45,6 +46,8 @@ int tc_prepare(doe_ctx* c, TcRes* r) {
 
 // The tensor-core passes cover 1024 x 1024 planes.
 bool tc_applies(const doe_ctx* c, int nx, int ny) { return c->tune_sweep_tc && nx == tcfft::kN && ny == tcfft::kN; }
+// Formulation of the CUDA-core sweep column pass (launch_sweep_col).
+int sweep_form(const doe_ctx* c) { return c->tune_sweep_hsym ? 2 : (c->tune_sweep_fused ? 1 : 0); }
 
 // Per-field spectrum maxima (zeroed), one unsigned per field.
 int tc_maxbits(doe_ctx* c, int nfields, unsigned** out) {
@@ -155,8 +158,7 @@ struct SweepPipe {
         } else {
           DOE_TRY(with_col(c, ny, kTuneSweep, [&](auto S) {
             const ColSweepBase b{{}, spec, w, tab, nx, ny, g0};
-            if (c->tune_sweep_fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, gn, nx);
-            return launch_col<decltype(S)>(c, ColSweep{b}, gn, nx);
+            return launch_sweep_col<decltype(S)>(c, b, gn, nx, sweep_form(c));
           }));
         }
         DOE_CUDA(c, cudaEventRecord(ev_col(g), c->stream));
@@ -280,7 +282,9 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
   Fnv k;
   k.val(d_fields);
   k.val(d_out);
-  for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused, c->tune_sweep_tc}) k.val(v);
+  for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused, c->tune_sweep_tc,
+                c->tune_sweep_hsym})
+    k.val(v);
   k.val(c->slot_gen);  // a reallocated scratch slot invalidates the captured addresses
   for (double v : {dx, dy, soft_edge}) k.val(v);
   k.val(c->tune_sweep_group);
@@ -460,7 +464,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
   const int lx = ilog2i(nx), ly = ilog2i(ny);
   int pick[4] = {0, 0, 0, 0};
   const int nrow = row_variant_count(nx), ncol = col_variant_count(ny);
-  float best_fused[2] = {1e30f, 1e30f};  // sweep column pass, per formulation
+  float best_fused[3] = {1e30f, 1e30f, 1e30f};  // sweep column pass, per formulation
   for (int kind : {(int)kTuneFft, (int)kTuneSweep}) {
     float best = 1e30f;
     for (int v = 0; v < nrow; ++v) {
@@ -481,14 +485,15 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     int best_f = 0;
     for (int v = 0; v < ncol; ++v) {
       c->tune_col[kind][ly] = (unsigned char)v;
-      for (int fused = 0; fused < (kind == kTuneSweep ? 2 : 1); ++fused) {
+      // sweep column pass formulations: 0 all reads first, 1 read and multiply per
+      // element, 2 transfer function shared between mirrored rows (sweep_sym.cuh)
+      for (int fused = 0; fused < (kind == kTuneSweep ? 3 : 1); ++fused) {
         float ms;
         DOE_TRY(time_variant(c, [&]() {
           return with_col(c, ny, kind, [&](auto S) {
             if (kind == kTuneSweep) {
               const ColSweepBase b{{}, spec, w, tab, nx, ny, 0};
-              if (fused) return launch_col<decltype(S)>(c, ColSweepFused{b}, planes, nx);
-              return launch_col<decltype(S)>(c, ColSweep{b}, planes, nx);
+              return launch_sweep_col<decltype(S)>(c, b, planes, nx, fused);
             }
             return launch_col<decltype(S)>(c, ColC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, nx);
           });
@@ -502,7 +507,10 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
       }
     }
     c->tune_col[kind][ly] = (unsigned char)pick[kind == kTuneFft ? 1 : 3];
-    if (kind == kTuneSweep) c->tune_sweep_fused = best_f;
+    if (kind == kTuneSweep) {
+      c->tune_sweep_fused = best_f == 1 ? 1 : 0;
+      c->tune_sweep_hsym = best_f == 2 ? 1 : 0;
+    }
   }
   // planes per launch pair of the pipelined sweep, and (for 1024^2 planes) the
   // tensor-core passes against the CUDA-core passes: time one 64-distance field
