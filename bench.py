@@ -43,11 +43,14 @@ BYTES_PER_PX = 16  # read complex64 spectrum + write complex64 output, per outpu
 SWEEP_PASSES = {"asm_sweep_col": "column", "tc_sweep_col": "column", "fft_row_inv": "row", "tc_sweep_row": "row"}
 
 
+TRAFFIC_RECORD = "traffic_sweep_1024.md"
+
+
 def recorded_traffic(kernel, planes_per_launch):
     """DRAM bytes of one launch of `kernel` (this many planes) from the committed
-    ncu capture record: rows `| kernel | dram bytes per plane | ... |` of
-    profiles/traffic_sweep_1024.md; None when the kernel has no record."""
-    path = os.path.join(ROOT, "profiles", "traffic_sweep_1024.md")
+    ncu capture record of the sweep passes (its table rows read `| kernel | dram
+    bytes per plane | ... |`); None when the kernel has no record."""
+    path = os.path.join(ROOT, "profiles", TRAFFIC_RECORD)
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -224,6 +227,9 @@ WGS_CONFIG = {"workload": "wgs256", "grid": [256, 256], "max_iterations": 100,
               "targets": "3-8 seeded rectangles 4-40 px in the central 128^2, autoRoi", "band_limit": False}
 
 
+DESIGN_TUNE = [True]  # --no-design-tune clears it
+
+
 def tune_wgs(ctx, n_designs, rank=0, trial_iterations=4):
     """Design-pass autotuning (doe_autotune_design) on this rank's own C1 batch,
     before any timing: shape variants of the passes and the cluster-resident loop."""
@@ -244,7 +250,7 @@ def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=
     on one."""
     import torch
     import torch.distributed as dist
-    tuning = tune_wgs(ctx, designs, rank)
+    tuning = tune_wgs(ctx, designs, rank) if DESIGN_TUNE[0] else None
     r = run_wgs(ctx, device, designs, max(warmup, 3), steps, goal=0.01, rank=rank)
     fixed = run_wgs(ctx, device, designs, 1, 1, rank=rank)
     ms, reached = r["ms_per_step"], r["reached"]
@@ -349,6 +355,12 @@ def measure_multiplane(ctx, device, warmup, steps, cpu, e2e_on, rank=0, world=1)
     d_ill, d_tgt, d_roi = f32(ill), f32(tgt).reshape(MP_B * P, n), f32(roi).reshape(MP_B * P, n)
     d_ph = torch.zeros((MP_B, n), dtype=torch.float32, device=device)
     res = {}
+    tuning = None
+    if DESIGN_TUNE[0]:  # the 2048-point design-pass shapes, timed on GS over plane 0 of each design
+        ch = batch.autotune_design(ctx, d_ill, f32(tgt[:, 0]), d_ph, nx=MP_N, ny=MP_N, dx=MP_DX, lam=MP_LAM,
+                                   z=MP_Z[0], iterations=MP_ITERS, algorithm="gs", trial_iterations=2)
+        tuning = {"row_variant": ch[0], "col_variant": ch[1],
+                  "tuner": "doe_autotune_design on gerchbergSaxton at 2048^2 (the multi-plane loop's passes)"}
 
     def step():
         d_ph.zero_()
@@ -404,7 +416,7 @@ def measure_multiplane(ctx, device, warmup, steps, cpu, e2e_on, rank=0, world=1)
         one = mp_cpu_baseline(threads=1)
         cb["single_core"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
     return {"metric": MP_METRIC, "value": value, "unit": "design-iterations/s", "ms_per_step": ms,
-            "config": MP_CONFIG, "roofline": roof,
+            "config": dict(MP_CONFIG, design_tuning=tuning), "roofline": roof,
             "final_error": {"median": float(np.median(err)), "max": float(err.max())},
             "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches}
 
@@ -510,6 +522,13 @@ def measure_uneven(ctx, device, warmup, steps, cpu, rank=0, world=1):
                         "iterations": UN_ITERS, "illumination": f32(ill), "target_amp": f32(tgt), "roi": f32(roi),
                         "phase": p0.clone()})
     m = batch.DesignMulti(ctx)
+    tuning = {}
+    if DESIGN_TUNE[0]:  # design-pass shapes per size class, on that class's own designs, before any timing
+        for cl in classes:
+            kw = {k: cl[k] for k in ("nx", "dx", "lam", "z", "algorithm", "iterations", "roi")}
+            ch = batch.autotune_design(ctx, cl["illumination"], cl["target_amp"], cl["phase"], ny=cl["nx"],
+                                       trial_iterations=3, **kw)
+            tuning[str(cl["nx"])] = {"row_variant": ch[0], "col_variant": ch[1]}
 
     def reset():
         for cl, p in zip(classes, ph0):
@@ -557,7 +576,7 @@ def measure_uneven(ctx, device, warmup, steps, cpu, rank=0, world=1):
     cb = uneven_cpu_baseline() if cpu else None
     m.close()
     return {"metric": UN_METRIC, "value": value, "unit": "designs/s", "ms_per_step": ms,
-            "config": dict(UN_CONFIG, counts={str(k): v for k, v in counts.items()}),
+            "config": dict(UN_CONFIG, counts={str(k): v for k, v in counts.items()}, design_tuning=tuning),
             "roofline": {"bound": "hbm", "kernel": "whole graph (column + row pass per iteration, all classes)",
                          "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bytes_ / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
@@ -901,10 +920,13 @@ def main():
                     help="profiling runs: skip the autotuner (its timings are distorted under a profiler) and set "
                          "these variants instead, e.g. fft_row=3,fft_col=0,sweep_row=3,sweep_col=4,sweep_fused=1,"
                          "sweep_group=64 (the choices the tuner makes on B200)")
+    ap.add_argument("--no-design-tune", action="store_true",
+                    help="skip doe_autotune_design before the design workloads (default shapes)")
     ap.add_argument("--fields", type=int, default=NFIELDS,
                     help="fields per step (profiling runs use fewer; the benchmark uses 64)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+    DESIGN_TUNE[0] = not args.no_design_tune
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -1032,7 +1054,7 @@ def main():
                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at "
                                        "full size, per plane, scaled to this launch's planes "
-                                       "(profiles/traffic_sweep_1024.md)") if traffic else None,
+                                       f"(profiles/{TRAFFIC_RECORD})") if traffic else None,
                     "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6, "launches": cnt,
                     "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()},
                     "per_kernel_note": "instrumented step with both passes on one stream (each launch timed alone)"}
