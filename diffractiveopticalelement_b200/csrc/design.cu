@@ -46,22 +46,10 @@ __global__ void design_init_kernel(DesignBufs b, int B, bool wgs) {
       b.st[d].best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
       b.st[d].eff_cur = 0.0;
       b.st[d].stop = -1;
-      b.st[d].pad = 0;
+      b.st[d].best_it = -2;
       b.st[d].sT = 0.0;
       b.st[d].sTT = 0.0;
     }
-  }
-}
-
-// Best-iterate snapshot after the last image-plane WGS iteration.
-__global__ void design_final_snapshot_kernel(DesignBufs b, int B, int it) {
-  const long n = b.pe();
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (long)B * n; i += (long)gridDim.x * blockDim.x) {
-    const long d = i / n;
-    if (!b.improved[d * b.iters + it]) continue;
-    const float2 u = b.U[i];
-    b.best_phase[i] = b.phase[i];
-    b.best_amp[i] = sqrtf(u.x * u.x + u.y * u.y);
   }
 }
 
@@ -209,8 +197,8 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   const int ntab = fourier ? 0 : (tab_shared ? 1 : B);
   const bool needU = wgs && !fourier;
   void *p0, *p1;
-  DOE_TRY(ensure_slot(c, kSlotDesign0, (size_t)(needU ? 2 : 1) * Bn * sizeof(float2) + (size_t)ntab * n * sizeof(float2) + 1024, &p0));
-  DOE_TRY(ensure_slot(c, kSlotDesign1, (size_t)4 * Bn * sizeof(float) + 1024, &p1));
+  DOE_TRY(ensure_slot(c, kSlotDesign0, (size_t)(needU ? 3 : 1) * Bn * sizeof(float2) + (size_t)ntab * n * sizeof(float2) + 1024, &p0));
+  DOE_TRY(ensure_slot(c, kSlotDesign1, (size_t)(needU ? 5 : 4) * Bn * sizeof(float) + 1024, &p1));
   char* q0 = (char*)p0;
   char* q1 = (char*)p1;
   DesignBufs b;
@@ -230,6 +218,7 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   b.phase = a->phase;
   b.W = (float2*)take(q0, Bn * sizeof(float2));
   b.U = needU ? (float2*)take(q0, Bn * sizeof(float2)) : nullptr;
+  b.U2 = needU ? (float2*)take(q0, Bn * sizeof(float2)) : nullptr;
   float2* htab = ntab ? (float2*)take(q0, (size_t)ntab * n * sizeof(float2)) : nullptr;
   b.htab = htab;
   b.htab_stride = ntab > 1 ? n : 0;
@@ -237,6 +226,7 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   b.wraw = wgs ? (float*)take(q1, Bn * sizeof(float)) : nullptr;
   b.best_phase = wgs ? (float*)take(q1, Bn * sizeof(float)) : nullptr;
   b.best_amp = wgs ? (float*)take(q1, Bn * sizeof(float)) : nullptr;
+  b.phase2 = needU ? (float*)take(q1, Bn * sizeof(float)) : nullptr;
   b.err_hist = a->error;
   b.eff_hist = a->efficiency;
   b.rmse_goal = a->rmse_goal;
@@ -259,12 +249,7 @@ extern "C" int doe_design_dev(doe_ctx* c, const doe_design_dev_desc* a) {
   if (!fourier && !wgs) {
     DOE_TRY(design_run_gs(c, b, B, I));
   } else if (!fourier) {
-    DOE_TRY(design_run_wgs(c, b, B, I));
-    {
-      LaunchScope ls(c, "design_snapshot");
-      design_final_snapshot_kernel<<<grid_for(Bn), 256, 0, c->stream>>>(b, B, I - 1);
-      DOE_CUDA(c, cudaGetLastError());
-    }
+    DOE_TRY(design_run_wgs(c, b, B, I));  // leaves the best iterates in best_phase / best_amp
     if (b.rmse_goal > 0 || a->iterations_used) {
       LaunchScope ls(c, "design_goal_out");
       design_goal_out_kernel<<<(B + 255) / 256, 256, 0, c->stream>>>(b, B, I, a->iterations_used);

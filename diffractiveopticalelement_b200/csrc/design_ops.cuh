@@ -19,7 +19,7 @@ struct DesignState {
   double best;      // WGS: best unweighted ROI RMSE so far
   double eff_cur;   // image-plane WGS: efficiency of the current forward field
   int stop;         // -1 running; else the iteration whose field met the screen goal
-  int pad;
+  int best_it;      // image-plane WGS (passes): the iteration of the best iterate (-2: none yet)
   double sT, sTT;   // screen goal: sum T over the plane, sum T^2 over the ROI (fixed)
 };
 
@@ -47,6 +47,8 @@ struct DesignBufs {
   float* amp;           // [B][n] amplitude of the current forward field
   float* best_amp;      // [B][n]
   float2* U;            // [B][n] target-plane field (image-plane WGS)
+  float2* U2;           // [B][n] image-plane WGS passes: second field buffer (even / odd iterations)
+  float* phase2;        // [B][n] image-plane WGS passes: second phase buffer
   float2* W;            // [B][n] work
   const float2* htab;   // transfer function in FFT bin order
   long htab_stride;     // elements between designs (0: shared geometry)
@@ -508,7 +510,10 @@ struct RowWgsTarget {
           imp = true;  // return the iterate that met the goal
         }
       }
-      if (imp) S.best = rmse;
+      if (imp) {
+        S.best = rmse;
+        S.best_it = it;
+      }
       b.improved[h] = imp ? 1 : 0;
       b.err_hist[h] = S.best;
       b.eff_hist[h] = S.eff_cur;
@@ -518,19 +523,28 @@ struct RowWgsTarget {
   }
 };
 
-// Image-plane WGS, start of an iteration (src/doe.js:380-397 with weights): load
-// the stored forward field U, apply the constraint with t * w_raw * norm inside the
-// ROI (outside: unchanged), forward row FFT of the back-propagation. When the
-// previous iteration improved the best RMSE, its phase and amplitude are copied
-// into the best-iterate buffers on the way.
+// Image-plane WGS, start of iteration `it` (src/doe.js:380-397 with weights): load
+// the forward field U of iteration it - 1, apply the constraint with
+// t * w_raw * norm inside the ROI (outside: unchanged), forward row FFT of the
+// back-propagation.
+//
+// Best iterate, kept lazily: the phase and field of iteration k live in one of two
+// alternating buffers each (phase produced by iteration k in buffer (k + 1) mod 2,
+// field in buffer k mod 2) until iteration k + 2 overwrites them. So the best
+// iterate needs no copy while later iterations keep improving on it; only when
+// the design's best is still iteration it - 2 when iteration it starts (it did not
+// improve since) does this pass copy that iterate's phase and amplitude into the
+// best-iterate buffers, from the buffers iteration it is about to overwrite. The
+// loop's last pass resolves where each design's best iterate ended up.
 struct RowWgsConstrain : NoReduce {
   static constexpr const char* kName = "design_row_wgs_constrain";
   static constexpr int kStages = 1;
   static constexpr bool kInv1 = false, kInv2 = false;
-  DesignBufs b;
-  int snap_it;  // -1: no snapshot check
-  // a stopped design runs this pass once more, for the snapshot of its last iterate
-  __device__ __forceinline__ bool skip(int p) const { return design_stopped(b.st, p) && b.st[p].stop != snap_it; }
+  DesignBufs b;             // b.U: the field of iteration it - 1
+  int it;
+  const float* ph_old;      // phase produced by iteration it - 2
+  const float2* u_old;      // field of iteration it - 2
+  __device__ __forceinline__ bool skip(int p) const { return design_stopped(b.st, p); }
   struct State {
     const float* t;
     const float* m;
@@ -538,6 +552,7 @@ struct RowWgsConstrain : NoReduce {
     const float2* U;
     float2* W;
     const float* ph;
+    const float2* uo;
     float* bph;
     float* bamp;
     float wn;
@@ -546,8 +561,8 @@ struct RowWgsConstrain : NoReduce {
   __device__ __forceinline__ State init(int p, int y) const {
     const long o = p * b.pe() + (long)y * b.nx;
     const long ot = p * b.tgt_stride + (long)y * b.nx;
-    const bool snap = snap_it >= 0 && b.improved[(long)p * b.iters + snap_it] != 0;
-    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, b.phase + o,
+    const bool snap = it >= 2 && b.st[p].best_it == it - 2;
+    return {b.tgt + ot, b.roi ? b.roi + ot : nullptr, b.wraw + o, b.U + o, b.W + o, ph_old + o, u_old + o,
             b.best_phase + o, b.best_amp + o, (float)b.st[p].norm, snap};
   }
   // every field read and side-plane prefetch of the thread first, then the
@@ -556,7 +571,10 @@ struct RowWgsConstrain : NoReduce {
     prefetch_l1(&s.t[x]);
     prefetch_l1(&s.w[x]);
     if (s.m) prefetch_l1(&s.m[x]);
-    if (s.snap) prefetch_l1(&s.ph[x]);
+    if (s.snap) {
+      prefetch_l1(&s.ph[x]);
+      prefetch_l1(&s.uo[x]);
+    }
     return __ldg(&s.U[x]);
   }
   __device__ __forceinline__ float2 finish_load(const State& s, int x, float2 u) const {
@@ -565,9 +583,9 @@ struct RowWgsConstrain : NoReduce {
     const float w = __ldg(&s.w[x]);
     const float a = sqrtf(u.x * u.x + u.y * u.y);
     if (s.snap) {
-      const float ph = __ldg(&s.ph[x]);
-      s.bph[x] = ph;
-      s.bamp[x] = a;
+      const float2 uo = __ldg(&s.uo[x]);
+      s.bph[x] = __ldg(&s.ph[x]);
+      s.bamp[x] = sqrtf(uo.x * uo.x + uo.y * uo.y);
     }
     if (m > 0.f && a > 0.f) return cscale(u, (t * (w * s.wn)) / a);
     return u;
