@@ -136,6 +136,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_tc;
   } else if (k == "sweep_hsym") {
     *value = c->tune_sweep_hsym;
+  } else if (k == "surrogate_tc") {
+    *value = c->tune_surrogate_tc;
   } else if (k == "design_cluster") {
     *value = (long long)c->tune_design_cluster;  // bit log2(n) set: n^2 runs cluster-resident
   } else {
@@ -161,6 +163,10 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   }
   if (k == "sweep_hsym") {
     c->tune_sweep_hsym = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "surrogate_tc") {
+    c->tune_surrogate_tc = value ? 1 : 0;
     return DOE_OK;
   }
   if (k == "design_cluster") {

@@ -492,7 +492,8 @@ int design_error_check(doe_ctx* c) {
   if (h) {
     DOE_CUDA(c, cudaMemset(c->slot[kSlotErr], 0, sizeof(int)));
     return set_err(c, DOE_ERR_TIMEOUT,
-                   "weightedGerchbergSaxton: a cluster barrier of the on-chip design loop gave up waiting (code %d)",
+                   "a bounded device wait gave up (code %d: 2 = a cluster barrier of the on-chip design loop, "
+                   "3 = an MMA of the surrogate's tensor-core convolution)",
                    h);
   }
   return DOE_OK;

@@ -18,6 +18,7 @@
 
 #include "engine.cuh"
 #include "unet_kernels.cuh"
+#include "unet_tc.cuh"
 
 using namespace doe;
 using namespace doe::unet;
@@ -295,19 +296,51 @@ int add_conv(doe_surrogate* s, int cin, int cout) {
   return (int)s->conv.size() - 1;
 }
 
+// One 3x3 convolution launch: the tcgen05 kernel where its shape rules hold
+// (kch input channels of the GEMM a multiple of 64, nout output channels a
+// multiple of 32) and the context allows it ("surrogate_tc"), else mma.sync.
+template <int BN, int S>
+int launch_conv_tc_s(doe_ctx* c, const ConvArgs& a, long P, int nout) {
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+  DOE_TRY(prepare_kernel(c, conv3x3_tc_kernel<BN, S>, ConvTc<BN, S>::SMEM, attr_set, false));
+  int* err;
+  DOE_TRY(design_error_word(c, &err));
+  conv3x3_tc_kernel<BN, S>
+      <<<dim3((unsigned)((P + 127) / 128), nout / BN), 128, ConvTc<BN, S>::SMEM, c->stream>>>(a, err);
+  DOE_CUDA(c, cudaGetLastError());
+  return DOE_OK;
+}
+// Three operand stages: deeper rings (4, 6) measured slower on B200 (2.36 ms
+// against 2.63 and 3.29 ms for the tensor-core layers of a 16-design 256^2
+// forward pass), the shared memory they take costing resident CTAs.
+template <int BN>
+int launch_conv_tc(doe_ctx* c, const ConvArgs& a, long P, int nout) {
+  return launch_conv_tc_s<BN, 3>(c, a, P, nout);
+}
+
+int conv_launch(doe_surrogate* s, const ConvArgs& a, int kch, int nout, const char* name, const char* tc_name) {
+  const long P = (long)a.B * a.H * a.W;
+  if (s->c->tune_surrogate_tc && kch % 64 == 0 && nout % 32 == 0) {
+    LaunchScope ls(s->c, tc_name);
+    if (nout % 128 == 0) return launch_conv_tc<128>(s->c, a, P, nout);
+    if (nout % 64 == 0) return launch_conv_tc<64>(s->c, a, P, nout);
+    return launch_conv_tc<32>(s->c, a, P, nout);
+  }
+  LaunchScope ls(s->c, name);
+  if (nout % 64 == 0) {
+    conv3x3_kernel<64><<<dim3((unsigned)((P + kBM - 1) / kBM), nout / 64), kConvThreads, 0, s->c->stream>>>(a);
+  } else {
+    conv3x3_kernel<32><<<dim3((unsigned)((P + kBM - 1) / kBM), nout / 32), kConvThreads, 0, s->c->stream>>>(a);
+  }
+  DOE_CUDA(s->c, cudaGetLastError());
+  return DOE_OK;
+}
+
 // conv(in -> out) with bias + ReLU; layer index li
 int conv_fwd(doe_surrogate* s, int li, int B, const bf16* in, int in_cs, bf16* out, int out_cs, int H, int W) {
   const ConvLayer& L = s->conv[li];
   ConvArgs a{in, in_cs, L.cin, L.wb, s->w + L.off_b, out, out_cs, L.cout, nullptr, 0, 1, B, H, W};
-  const long P = (long)B * H * W;
-  LaunchScope ls(s->c, "unet_conv_fwd");
-  if (L.cout % 64 == 0) {
-    conv3x3_kernel<64><<<dim3((unsigned)((P + kBM - 1) / kBM), L.cout / 64), kConvThreads, 0, s->c->stream>>>(a);
-  } else {
-    conv3x3_kernel<32><<<dim3((unsigned)((P + kBM - 1) / kBM), L.cout / 32), kConvThreads, 0, s->c->stream>>>(a);
-  }
-  DOE_CUDA(s->c, cudaGetLastError());
-  return DOE_OK;
+  return conv_launch(s, a, L.cin, L.cout, "unet_conv_fwd", "unet_conv_fwd_tc");
 }
 
 // input gradient: dIn = conv(dOut, flipped W^T), masked by `mask` (> 0) when given
@@ -315,15 +348,7 @@ int conv_dgrad(doe_surrogate* s, int li, int B, const bf16* dout, int dout_cs, b
                const bf16* mask, int mask_cs, int H, int W) {
   const ConvLayer& L = s->conv[li];
   ConvArgs a{dout, dout_cs, L.cout, L.wt, nullptr, din, din_cs, L.cin, mask, mask_cs, 0, B, H, W};
-  const long P = (long)B * H * W;
-  LaunchScope ls(s->c, "unet_conv_dgrad");
-  if (L.cin % 64 == 0) {
-    conv3x3_kernel<64><<<dim3((unsigned)((P + kBM - 1) / kBM), L.cin / 64), kConvThreads, 0, s->c->stream>>>(a);
-  } else {
-    conv3x3_kernel<32><<<dim3((unsigned)((P + kBM - 1) / kBM), L.cin / 32), kConvThreads, 0, s->c->stream>>>(a);
-  }
-  DOE_CUDA(s->c, cudaGetLastError());
-  return DOE_OK;
+  return conv_launch(s, a, L.cout, L.cin, "unet_conv_dgrad", "unet_conv_dgrad_tc");
 }
 
 int conv_wgrad(doe_surrogate* s, int li, int B, const bf16* in, int in_cs, const bf16* dout, int dout_cs, int H,

@@ -83,12 +83,14 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * distributed shared memory) instead of five passes per iteration, 0 for the
  * passes on all three (default), or (log2(n) << 8) | on for one grid size;
  * its current value reads back as a mask with bit log2(n) set per size on;
+ * "surrogate_tc" = 0 to run every surrogate convolution on the mma.sync kernels
+ * instead of tcgen05 where the layer allows (default 1);
  * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
 /* Current value of "sweep_group", "sweep_fused", "sweep_graph", "sweep_hsym",
- * "sweep_tc" or "design_cluster". */
+ * "sweep_tc", "design_cluster" or "surrogate_tc". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for

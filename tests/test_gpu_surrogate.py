@@ -138,3 +138,42 @@ def test_supervised_gradient(engine):
     d = a.astype(np.float64) - b
     assert abs(loss.item() - np.mean(1 - np.cos(d))) < 1e-6
     assert np.max(np.abs(g.cpu().numpy() - np.sin(d) / d.size)) < 1e-9
+
+
+@pytest.mark.parametrize("n,base,levels,B", [(64, 32, 4, 3), (32, 64, 3, 2)])
+def test_tensor_core_convolutions_match_the_mma_sync_ones(engine, n, base, levels, B):
+    """The tcgen05 convolution (layers whose GEMM input has a multiple of 64
+    channels, forward and input gradient) against the mma.sync kernel on the same
+    weights and inputs: both accumulate in FP32 and round to BF16, so they agree up
+    to BF16 rounding of differently ordered sums."""
+    import ctypes as C
+    import torch
+    from diffractiveopticalelement_b200 import _lib
+    from diffractiveopticalelement_b200.surrogate import Surrogate
+    irr, roi = _inputs(n, B, 5 + n)
+    rng = np.random.default_rng(9)
+    dphase = rng.standard_normal((B, n * n)).astype(np.float32)
+    res = {}
+    for tc in (1, 0):
+        ctx = _lib.Context(0)
+        ctx.check(ctx.lib.doe_ctx_set_tuning(ctx.h, b"surrogate_tc", tc))
+        ctx.check(ctx.lib.doe_ctx_set_profiling(ctx.h, 1))
+        s = Surrogate(n=n, base=base, levels=levels, max_batch=B, seed=11, ctx=ctx)
+        ph = s.forward(torch.tensor(irr, device="cuda"), torch.tensor(roi, device="cuda")).cpu().numpy()
+        s.zero_grad()
+        s.backward(torch.tensor(dphase, device="cuda"))
+        g = s.gradients().astype(np.float64)
+        ctx.synchronize()
+        names = C.create_string_buffer(64 * 64)
+        ms, cnt = (C.c_double * 64)(), (C.c_ulonglong * 64)()
+        k = ctx.lib.doe_ctx_profile_read(ctx.h, 64, names, 64, ms, cnt)
+        labels = {names.raw[64 * q:64 * (q + 1)].split(b"\0")[0].decode() for q in range(k)}
+        res[tc] = (ph, g, labels)
+        s.close()
+        ctx.close()
+    assert {"unet_conv_fwd_tc", "unet_conv_dgrad_tc"} <= res[1][2]
+    assert "unet_conv_fwd_tc" not in res[0][2]
+    (p1, g1, _), (p0, g0, _) = res[1], res[0]
+    print("phase rel", rel_l2(np.exp(1j * p1), np.exp(1j * p0)), "grad rel", rel_l2(g1, g0))
+    assert rel_l2(np.exp(1j * p1), np.exp(1j * p0)) < 1e-2
+    assert rel_l2(g1, g0) < 5e-2
