@@ -166,7 +166,8 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
     return DOE_OK;
   }
   if (k == "surrogate_tc") {
-    c->tune_surrogate_tc = value ? 1 : 0;
+    if (value < 0 || value > 3) return set_err(c, DOE_ERR_BAD_ARG, "surrogate_tc must be in [0, 3]");
+    c->tune_surrogate_tc = (int)value;
     return DOE_OK;
   }
   if (k == "design_cluster") {

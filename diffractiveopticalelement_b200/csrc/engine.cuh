@@ -56,7 +56,8 @@ struct doe_ctx {
   int tune_sweep_hsym = 0;             // 1: sweep column pass shares H between mirrored rows
   int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
   unsigned tune_design_cluster = 0;    // bit log2(n): square n^2 image-plane WGS runs cluster-resident
-  int tune_surrogate_tc = 1;           // 1: surrogate convolutions with cin % 64 == 0 run on tcgen05
+  int tune_surrogate_tc = 2;           // surrogate convolutions with cin % 64 == 0: 0 mma.sync, 1 tcgen05
+                                       // with cp.async operands, 2 / 3 tcgen05 with TMA operands (4 / 3 stages)
   void* tc_tables = nullptr;           // tensor-core tables built in this slot allocation
   int num_sms = 0;
   unsigned long long slot_gen = 0;     // bumped whenever a scratch slot is reallocated

@@ -83,8 +83,10 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * distributed shared memory) instead of five passes per iteration, 0 for the
  * passes on all three (default), or (log2(n) << 8) | on for one grid size;
  * its current value reads back as a mask with bit log2(n) set per size on;
- * "surrogate_tc" = 0 to run every surrogate convolution on the mma.sync kernels
- * instead of tcgen05 where the layer allows (default 1);
+ * "surrogate_tc" selects the surrogate's convolution kernel where the layer
+ * allows tcgen05 (a multiple of 64 input channels): 0 mma.sync, 1 tcgen05 with
+ * cp.async operand staging, 2 tcgen05 with TMA operand staging and a 4-stage ring
+ * (default), 3 the same with 3 stages;
  * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */

@@ -140,12 +140,14 @@ def test_supervised_gradient(engine):
     assert np.max(np.abs(g.cpu().numpy() - np.sin(d) / d.size)) < 1e-9
 
 
-@pytest.mark.parametrize("n,base,levels,B", [(64, 32, 4, 3), (32, 64, 3, 2)])
+@pytest.mark.parametrize("n,base,levels,B", [(64, 32, 4, 3), (32, 64, 3, 2), (256, 32, 4, 2)])
 def test_tensor_core_convolutions_match_the_mma_sync_ones(engine, n, base, levels, B):
-    """The tcgen05 convolution (layers whose GEMM input has a multiple of 64
+    """The tcgen05 convolutions (layers whose GEMM input has a multiple of 64
     channels, forward and input gradient) against the mma.sync kernel on the same
-    weights and inputs: both accumulate in FP32 and round to BF16, so they agree up
-    to BF16 rounding of differently ordered sums."""
+    weights and inputs: operands staged by cp.async ("surrogate_tc" 1) or by the
+    tensor memory accelerator with a 4- or 6-stage ring (2, 3). All accumulate in
+    FP32 in the same K order and round to BF16 once; they agree bitwise in practice,
+    and are held here to BF16 rounding of differently ordered sums."""
     import ctypes as C
     import torch
     from diffractiveopticalelement_b200 import _lib
@@ -154,7 +156,7 @@ def test_tensor_core_convolutions_match_the_mma_sync_ones(engine, n, base, level
     rng = np.random.default_rng(9)
     dphase = rng.standard_normal((B, n * n)).astype(np.float32)
     res = {}
-    for tc in (1, 0):
+    for tc in (0, 1, 2, 3):
         ctx = _lib.Context(0)
         ctx.check(ctx.lib.doe_ctx_set_tuning(ctx.h, b"surrogate_tc", tc))
         ctx.check(ctx.lib.doe_ctx_set_profiling(ctx.h, 1))
@@ -171,9 +173,11 @@ def test_tensor_core_convolutions_match_the_mma_sync_ones(engine, n, base, level
         res[tc] = (ph, g, labels)
         s.close()
         ctx.close()
-    assert {"unet_conv_fwd_tc", "unet_conv_dgrad_tc"} <= res[1][2]
     assert "unet_conv_fwd_tc" not in res[0][2]
-    (p1, g1, _), (p0, g0, _) = res[1], res[0]
-    print("phase rel", rel_l2(np.exp(1j * p1), np.exp(1j * p0)), "grad rel", rel_l2(g1, g0))
-    assert rel_l2(np.exp(1j * p1), np.exp(1j * p0)) < 1e-2
-    assert rel_l2(g1, g0) < 5e-2
+    p0, g0, _ = res[0]
+    for tc in (1, 2, 3):
+        p1, g1, labels = res[tc]
+        assert {"unet_conv_fwd_tc", "unet_conv_dgrad_tc"} <= labels
+        print(f"surrogate_tc={tc}: phase rel", rel_l2(np.exp(1j * p1), np.exp(1j * p0)), "grad rel", rel_l2(g1, g0))
+        assert rel_l2(np.exp(1j * p1), np.exp(1j * p0)) < 1e-2
+        assert rel_l2(g1, g0) < 5e-2
