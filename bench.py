@@ -265,6 +265,10 @@ def measure_wgs(ctx, device, designs, warmup, steps, surrogate_steps, cpu, rank=
     if roof:
         roof["basis"] = ("dominant pass of the fixed 100-iteration loop (every design active): bytes per pixel x "
                          "designs x 256^2 over its average launch time")
+        # FFT arithmetic of the fixed loop: 4 2-D FFTs per iteration at 5 N^2 log2(N^2) FLOP each
+        flop = 20.0 * WGS_N * WGS_N * np.log2(WGS_N * WGS_N) * WGS_ITERS * designs
+        roof["fft_tflops"] = flop / (fixed["ms_per_step"] / 1e3) / 1e12
+        roof["fft_basis"] = "20 N^2 log2(N^2) FLOP per WGS iteration (4 2-D FFTs), fixed 100-iteration loop"
     out = {"metric": WGS_METRIC, "value": reached / (ms / 1e3), "unit": "designs/s", "ms_per_step": ms,
            "config": dict(WGS_CONFIG, designs=designs, design_tuning=tuning), "roofline": roof, "wgs256": r,
            "fixed_100_iterations": fixed, "gpu_launches": int(r["gpu_launches_per_step"] * steps)}
