@@ -1,5 +1,6 @@
 // context.cu -- context lifetime, twiddle tables and host helpers of the C ABI.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "engine.cuh"
@@ -162,7 +163,8 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
     return DOE_OK;
   }
   if (k == "sweep_hsym") {
-    c->tune_sweep_hsym = value ? 1 : 0;
+    if (value < 0 || value > 2) return set_err(c, DOE_ERR_BAD_ARG, "sweep_hsym must be 0, 1 or 2");
+    c->tune_sweep_hsym = (int)value;
     return DOE_OK;
   }
   if (k == "surrogate_tc") {
@@ -214,3 +216,20 @@ extern "C" int doe_host_free(doe_ctx* c, void* ptr) {
   DOE_CUDA(c, cudaFreeHost(ptr));
   return DOE_OK;
 }
+
+namespace doe {
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      (void)cudaGetLastError();
+  });
+  return fn;
+}
+}  // namespace doe

@@ -493,7 +493,7 @@ int design_error_check(doe_ctx* c) {
     DOE_CUDA(c, cudaMemset(c->slot[kSlotErr], 0, sizeof(int)));
     return set_err(c, DOE_ERR_TIMEOUT,
                    "a bounded device wait gave up (code %d: 2 = a cluster barrier of the on-chip design loop, "
-                   "3 = an MMA of the surrogate's tensor-core convolution)",
+                   "3 = an MMA of the surrogate's tensor-core convolution, 4 = a TMA copy of the sweep column pass)",
                    h);
   }
   return DOE_OK;

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cudaTypedefs.h>
+
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -112,6 +114,11 @@ int tc_check(doe_ctx* c);
 // design_error_check reads and clears it once the context's streams are synchronised.
 int design_error_word(doe_ctx* c, int** out);
 int design_error_check(doe_ctx* c);
+
+// cuTensorMapEncodeTiled (the TMA descriptor encoder), fetched once through the
+// runtime's driver entry point so that the library needs no link to libcuda;
+// null when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder();
 
 inline int check_grid(doe_ctx* c, int nx, int ny, const char* who) {
   if (!is_pow2(nx) || !is_pow2(ny))

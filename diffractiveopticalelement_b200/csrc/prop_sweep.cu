@@ -47,7 +47,9 @@ int tc_prepare(doe_ctx* c, TcRes* r) {
 // The tensor-core passes cover 1024 x 1024 planes.
 bool tc_applies(const doe_ctx* c, int nx, int ny) { return c->tune_sweep_tc && nx == tcfft::kN && ny == tcfft::kN; }
 // Formulation of the CUDA-core sweep column pass (launch_sweep_col).
-int sweep_form(const doe_ctx* c) { return c->tune_sweep_hsym ? 2 : (c->tune_sweep_fused ? 1 : 0); }
+int sweep_form(const doe_ctx* c) {
+  return c->tune_sweep_hsym == 2 ? 3 : (c->tune_sweep_hsym ? 2 : (c->tune_sweep_fused ? 1 : 0));
+}
 
 // Per-field spectrum maxima (zeroed), one unsigned per field.
 int tc_maxbits(doe_ctx* c, int nfields, unsigned** out) {
@@ -245,7 +247,8 @@ extern "C" int doe_asm_sweep(doe_ctx* c, const double* re, const double* im, int
   DOE_TRY(download_f64(c, out_re, ore, n * nz));
   DOE_TRY(download_f64(c, out_im, oim, n * nz));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
-  return tc_check(c);
+  DOE_TRY(tc_check(c));
+  return design_error_check(c);  // a TMA-staged column pass that gave up waiting
 }
 
 namespace {
@@ -464,7 +467,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
   const int lx = ilog2i(nx), ly = ilog2i(ny);
   int pick[4] = {0, 0, 0, 0};
   const int nrow = row_variant_count(nx), ncol = col_variant_count(ny);
-  float best_fused[3] = {1e30f, 1e30f, 1e30f};  // sweep column pass, per formulation
+  float best_fused[4] = {1e30f, 1e30f, 1e30f, 1e30f};  // sweep column pass, per formulation
   for (int kind : {(int)kTuneFft, (int)kTuneSweep}) {
     float best = 1e30f;
     for (int v = 0; v < nrow; ++v) {
@@ -486,8 +489,9 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     for (int v = 0; v < ncol; ++v) {
       c->tune_col[kind][ly] = (unsigned char)v;
       // sweep column pass formulations: 0 all reads first, 1 read and multiply per
-      // element, 2 transfer function shared between mirrored rows (sweep_sym.cuh)
-      for (int fused = 0; fused < (kind == kTuneSweep ? 3 : 1); ++fused) {
+      // element, 2 transfer function shared between mirrored rows (sweep_sym.cuh),
+      // 3 the same with the spectrum tile staged by TMA
+      for (int fused = 0; fused < (kind == kTuneSweep ? 4 : 1); ++fused) {
         float ms;
         DOE_TRY(time_variant(c, [&]() {
           return with_col(c, ny, kind, [&](auto S) {
@@ -509,7 +513,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     c->tune_col[kind][ly] = (unsigned char)pick[kind == kTuneFft ? 1 : 3];
     if (kind == kTuneSweep) {
       c->tune_sweep_fused = best_f == 1 ? 1 : 0;
-      c->tune_sweep_hsym = best_f == 2 ? 1 : 0;
+      c->tune_sweep_hsym = best_f == 2 ? 1 : (best_f == 3 ? 2 : 0);
     }
   }
   // planes per launch pair of the pipelined sweep, and (for 1024^2 planes) the

@@ -16,10 +16,6 @@
 #include <cstring>
 #include <vector>
 
-#include <cudaTypedefs.h>
-
-#include <mutex>
-
 #include "engine.cuh"
 #include "unet_kernels.cuh"
 #include "unet_tc.cuh"
@@ -320,22 +316,6 @@ int launch_conv_tc_s(doe_ctx* c, const ConvArgs& a, long P, int nout) {
 template <int BN>
 int launch_conv_tc(doe_ctx* c, const ConvArgs& a, long P, int nout) {
   return launch_conv_tc_s<BN, 3>(c, a, P, nout);
-}
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda).
-PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    else
-      (void)cudaGetLastError();
-  });
-  return fn;
 }
 
 // TMA-fed tcgen05 form; DOE_ERR_UNSUPPORTED when the layer's layout does not fit

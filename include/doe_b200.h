@@ -75,7 +75,8 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * element in the sweep column pass (0: all reads first); "sweep_graph" = 0 to
  * disable CUDA-graph replay of repeated device sweeps; "sweep_hsym" = 1 to have
  * the sweep column pass evaluate the transfer function once per pair of mirrored
- * rows (H depends on fy^2) into shared memory; "sweep_tc" = 0 to run
+ * rows (H depends on fy^2) into shared memory, 2 to also have its spectrum tile
+ * staged into shared memory by TMA; "sweep_tc" = 0 to run
  * 1024 x 1024 focus sweeps on the FP32 CUDA-core passes instead of the tcgen05
  * tensor-core passes (default 1); "design_cluster" = 1 to run image-plane
  * weightedGerchbergSaxton on square 64^2, 128^2 and 256^2 grids as one

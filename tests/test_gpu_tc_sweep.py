@@ -138,16 +138,20 @@ def test_replayed_sweep_after_scratch_growth(engine):
 
 def test_mirrored_row_transfer_function_form(engine, oracle):
     """The sweep column pass that evaluates H once per pair of mirrored rows
-    (H(kx, ky) = H(kx, N - ky)) gives the plain pass's planes and the oracle's."""
+    (H(kx, ky) = H(kx, N - ky)), with per-element spectrum reads ("sweep_hsym" 1) or
+    the CTA's spectrum tile staged by TMA (2), gives the plain pass's planes and the
+    oracle's."""
     f = smooth_field(N, DX, 41)[None]
     zs = np.array([0.017, 0.029, 0.046])
     outs = {}
-    for hsym in (0, 1):
+    for hsym in (0, 1, 2):
         ctx = make_ctx(engine, 0, graph=0)
         ctx.check(ctx.lib.doe_ctx_set_tuning(ctx.h, b"sweep_hsym", hsym))
         outs[hsym] = sweep(ctx, f, np.array([532e-9]), zs)
         ctx.close()
-    print("mirrored-row form bitwise equal to the plain form:", np.array_equal(outs[0], outs[1]))
+    print("mirrored-row forms bitwise equal to the plain form:", np.array_equal(outs[0], outs[1]),
+          np.array_equal(outs[0], outs[2]))
     assert np.array_equal(outs[1], outs[0])  # the same factors, read from shared memory
+    assert np.array_equal(outs[2], outs[0])  # ... and the spectrum staged by TMA
     for k in (0, 2):
-        assert rel_l2(outs[1][k].ravel(), oracle_plane(oracle, f[0], 532e-9, zs[k])) < 1e-5
+        assert rel_l2(outs[2][k].ravel(), oracle_plane(oracle, f[0], 532e-9, zs[k])) < 1e-5
