@@ -1,7 +1,7 @@
 // unet.cu -- the warm-start surrogate: a 4-level U-Net (32-256 channels by
 // default) mapping a target irradiance (+ ROI) to a DOE phase, with its own BF16
 // forward, backward and Adam kernels. No counterpart in the reference; the
-// phase it predicts is only a starting point that WGS refines and judges.
+// phase it predicts is only a starting point that WGS refines and scores.
 //
 // Graph (all 3x3 convolutions with bias + ReLU; C_l = base << l):
 //   enc l < L-1 : a_l = conv(in_l, C_l); cat_l[:, 0:C_l] = conv(a_l, C_l); in_{l+1} = avgpool2(cat_l[:, 0:C_l])

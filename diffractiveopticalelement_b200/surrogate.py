@@ -1,7 +1,7 @@
 """Warm-start surrogate for image-plane WGS (no reference counterpart).
 
 A U-Net maps a target irradiance (and its ROI) to a DOE phase; WGS then refines
-that phase and judges the final screen RMSE (src/projector.js:554-595), so the
+that phase and decides the final screen RMSE (src/projector.js:554-595), so the
 network only ever replaces the random starting phase of src/doe.js:81-86. All
 network arithmetic runs in the engine's own BF16 kernels (csrc/unet.cu): the
 forward pass, the backward pass and Adam. Two training signals are provided:

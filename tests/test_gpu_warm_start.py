@@ -14,8 +14,8 @@ targets:
   * as a WGS start it is measured, not assumed: the screen RMSE after one and
     after up to 100 iterations (goal 2 %) and the iterations to the goal, warm
     against plain, are printed as they come out, and the warm designs must end
-    within 1.5x of the plain ones' median screen RMSE, since plain WGS remains the
-    judge of the final screen. Measured on B200: intensity loss 0.56 warm against
+    within 1.5x of the plain ones' median screen RMSE, since plain WGS still decides
+    the final screen. Measured on B200: intensity loss 0.56 warm against
     0.96 plain before WGS; after one iteration the warm starts are worse (screen
     RMSE 0.311 against 0.279: the smooth predicted phase lacks the speckle-scale
     diversity WGS feeds on), yet they reach 2 % sooner (median 24 iterations
