@@ -9,7 +9,9 @@
 //   weight gradient          : dW[Cout][9 Cin] = dOut^T[Cout][pixels] * im2col(in)
 // The input gradient is the forward convolution of dOut with the flipped,
 // channel-transposed kernel. Operand tiles are staged in shared memory with
-// cp.async (zero-filled halo) and fed to the MMAs with ldmatrix.
+// cp.async (zero-filled halo) and fed to the MMAs with ldmatrix. Layers whose
+// GEMM input has a multiple of 64 channels run the same GEMM on tcgen05 instead
+// (unet_tc.cuh); these kernels serve the 32-channel layers and the weight gradient.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
