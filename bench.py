@@ -997,9 +997,12 @@ def main():
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_graph", C.byref(graph)))
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_hsym", C.byref(hsym)))
     ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_tc", C.byref(tc)))
+    res = C.c_longlong(1)
+    ctx.check(L.doe_ctx_get_tuning(ctx.h, b"sweep_res", C.byref(res)))
     tuned = {"fft_row": chosen[0], "fft_col": chosen[1], "sweep_row": chosen[2], "sweep_col": chosen[3],
              "sweep_group": chosen[4], "sweep_fused_load": int(fused.value), "sweep_mirror_h": int(hsym.value),
-             "sweep_tensor_core": int(tc.value), "sweep_graph": int(graph.value)}
+             "sweep_tensor_core": int(tc.value), "sweep_graph": int(graph.value),
+             "sweep_resident_planes": int(res.value)}
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         step()

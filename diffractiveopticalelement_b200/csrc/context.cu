@@ -137,6 +137,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_tc;
   } else if (k == "sweep_hsym") {
     *value = c->tune_sweep_hsym;
+  } else if (k == "sweep_res") {
+    *value = c->tune_sweep_res;
   } else if (k == "surrogate_tc") {
     *value = c->tune_surrogate_tc;
   } else if (k == "design_cluster") {
@@ -160,6 +162,11 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   }
   if (k == "sweep_tc") {
     c->tune_sweep_tc = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "sweep_res") {
+    if (value < 1 || value > 64) return set_err(c, DOE_ERR_BAD_ARG, "sweep_res must be in [1, 64]");
+    c->tune_sweep_res = (int)value;
     return DOE_OK;
   }
   if (k == "sweep_hsym") {

@@ -56,6 +56,7 @@ struct doe_ctx {
   unsigned long long sweep_key = 0, sweep_pending = 0, sweep_launches = 0;
   int tune_sweep_fused = 0;            // 1: sweep column pass reads and multiplies per element
   int tune_sweep_hsym = 0;             // 1: sweep column pass shares H between mirrored rows
+  int tune_sweep_res = 1;              // > 1: planes per CTA over a spectrum tile staged once by TMA
   int tune_sweep_tc = 1;               // 1: 1024^2 sweeps run the tcgen05 tensor-core passes
   unsigned tune_design_cluster = 0;    // bit log2(n): square n^2 image-plane WGS runs cluster-resident
   int tune_surrogate_tc = 2;           // surrogate convolutions with cin % 64 == 0: 0 mma.sync, 1 tcgen05

@@ -286,7 +286,7 @@ extern "C" int doe_asm_sweep_dev(doe_ctx* c, const void* d_fields, int nfields, 
   k.val(d_fields);
   k.val(d_out);
   for (int v : {nfields, nx, ny, nz, band_limit, evanescent, c->tune_sweep_fused, c->tune_sweep_tc,
-                c->tune_sweep_hsym})
+                c->tune_sweep_hsym, c->tune_sweep_res})
     k.val(v);
   k.val(c->slot_gen);  // a reallocated scratch slot invalidates the captured addresses
   for (double v : {dx, dy, soft_edge}) k.val(v);
@@ -490,19 +490,21 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
       c->tune_col[kind][ly] = (unsigned char)v;
       // sweep column pass formulations: 0 all reads first, 1 read and multiply per
       // element, 2 transfer function shared between mirrored rows (sweep_sym.cuh),
-      // 3 the same with the spectrum tile staged by TMA
-      for (int fused = 0; fused < (kind == kTuneSweep ? 4 : 1); ++fused) {
+      // 3 the same with the spectrum tile staged by TMA, 4..6 the spectrum tile
+      // resident in shared memory across 2, 4 or 8 planes
+      for (int fused = 0; fused < (kind == kTuneSweep ? 7 : 1); ++fused) {
         float ms;
+        c->tune_sweep_res = fused >= 4 ? 2 << (fused - 4) : 1;
         DOE_TRY(time_variant(c, [&]() {
           return with_col(c, ny, kind, [&](auto S) {
             if (kind == kTuneSweep) {
               const ColSweepBase b{{}, spec, w, tab, nx, ny, 0};
-              return launch_sweep_col<decltype(S)>(c, b, planes, nx, fused);
+              return launch_sweep_col<decltype(S)>(c, b, planes, nx, fused < 4 ? fused : 1);
             }
             return launch_col<decltype(S)>(c, ColC64<true>{{}, w, w, nx, ny, pe, pe, 1.f}, planes, nx);
           });
         }, &ms));
-        if (kind == kTuneSweep) best_fused[fused] = std::min(best_fused[fused], ms);
+        if (kind == kTuneSweep && fused < 4) best_fused[fused] = std::min(best_fused[fused], ms);
         if (ms < best) {
           best = ms;
           best_f = fused;
@@ -514,6 +516,7 @@ extern "C" int doe_autotune(doe_ctx* c, int nx, int ny, double dx, double dy, do
     if (kind == kTuneSweep) {
       c->tune_sweep_fused = best_f == 1 ? 1 : 0;
       c->tune_sweep_hsym = best_f == 2 ? 1 : (best_f == 3 ? 2 : 0);
+      c->tune_sweep_res = best_f >= 4 ? 2 << (best_f - 4) : 1;
     }
   }
   // planes per launch pair of the pipelined sweep, and (for 1024^2 planes) the

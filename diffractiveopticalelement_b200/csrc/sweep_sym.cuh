@@ -164,11 +164,115 @@ inline int launch_sweep_tma(doe_ctx* c, const ColSweepBase& op, int nplanes, int
   return DOE_OK;
 }
 
+// Spectrum tile resident across planes: all planes of a field share one spectrum,
+// so a CTA has the TMA copy its C-column tile into shared memory once (32 KB at
+// 1024 x 4) and then runs K planes over it -- x H of plane k, inverse column FFT,
+// store -- reading the spectrum from shared memory each time. The spectrum then
+// crosses L2 once per K planes instead of once per plane, and no plane's transform
+// waits on global loads of it. Same bounded wait as the TMA-staged form.
+template <class S>
+constexpr int sweep_res_smem() {
+  return 128 + S::N * S::C * (int)sizeof(float2) + S::SMEM + 16;
+}
+
+template <class S>
+__global__ void __launch_bounds__(S::THREADS, S::MINB)
+    sweep_col_res_kernel(const __grid_constant__ CUtensorMap spec_map, ColSweepBase op,
+                         const float2* __restrict__ tw, int ncols, int nplanes, int K, int* __restrict__ err) {
+  using P = typename S::Plan;
+  constexpr int C = S::C, RMAX = P::RMAX, N = P::N, BOX = N < 256 ? N : 256;
+  extern __shared__ unsigned char smraw[];
+  float2* tile = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+  float2* scratch = tile + N * C;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(scratch) + S::SMEM);
+  const int c = threadIdx.x % C;
+  const int t = threadIdx.x / C;
+  const int x0 = blockIdx.x * C;
+  const int line = x0 + c;
+  const bool active = line < ncols;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+                 "r"((uint32_t)(N * C * sizeof(float2)))
+                 : "memory");
+#pragma unroll 1
+    for (int r0 = 0; r0 < N; r0 += BOX)
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+              tc::smem_u32(tile + r0 * C)),
+          "l"(reinterpret_cast<uint64_t>(&spec_map)), "r"(2 * x0), "r"(r0), "r"(tc::smem_u32(bar))
+          : "memory");
+  }
+  __syncthreads();
+  bool ok = tc::mbar_wait_bounded(bar, 0, 1000000000ull);
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, 4);
+      (void)tc::mbar_wait_bounded(bar, 0, 1000000000ull);
+    }
+    __syncthreads();
+    return;
+  }
+  SmemVec s{scratch, C, c};
+  const int p0 = blockIdx.y * K;
+#pragma unroll 1
+  for (int k = 0; k < K && p0 + k < nplanes; ++k) {
+    const auto st = op.init(p0 + k, active ? line : 0);
+    float2 v[RMAX];
+#pragma unroll
+    for (int q = 0; q < RMAX; ++q) {
+      const int ky = in_elem<P>(t, q);
+      v[q] = cmul(tile[ky * C + c], asm_h_col(st.h, op.tab, ky));
+    }
+    fft_run<P, true>(v, t, s, tw, BlockSync{});
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < RMAX; ++q) st.out[(long)out_elem<P>(t, q) * op.nx] = v[q];
+    }
+    __syncthreads();  // the scratch is reused by the next plane
+  }
+}
+
+template <class S>
+inline int launch_sweep_res(doe_ctx* c, const ColSweepBase& op, int nplanes, int ncols, int K) {
+  constexpr int smem = sweep_res_smem<S>();
+  if (smem > 200 * 1024 || (ncols % S::C) || (S::C * 8) % 16 || K < 1) return DOE_ERR_UNSUPPORTED;
+  const auto enc = tmap_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(op.spec) & 15)) return DOE_ERR_UNSUPPORTED;
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * op.nx, (cuuint64_t)op.ny};
+  const cuuint64_t strides[1] = {(cuuint64_t)op.nx * sizeof(float2)};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * S::C), (cuuint32_t)(S::N < 256 ? S::N : 256)}, es[2] = {1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(op.spec), dims, strides, box, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return DOE_ERR_UNSUPPORTED;
+  static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+  DOE_TRY(prepare_kernel(c, sweep_col_res_kernel<S>, smem, attr_set, false));
+  if (nplanes <= 0) return DOE_OK;
+  const int gy = (nplanes + K - 1) / K;
+  if (gy > 65535) return set_err(c, DOE_ERR_UNSUPPORTED, "column pass: too many plane groups per launch");
+  int* err;
+  DOE_TRY(design_error_word(c, &err));
+  LaunchScope ls(c, ColSweepBase::kName);
+  sweep_col_res_kernel<S><<<dim3(ncols / S::C, gy), S::THREADS, smem, c->stream>>>(map, op, c->tw + S::N, ncols,
+                                                                                     nplanes, K, err);
+  DOE_CUDA(c, cudaGetLastError());
+  return DOE_OK;
+}
+
 // The mirrored-row forms where they fit one SM's shared memory with room to spare
 // (lengths 16..4096): 2 with per-element spectrum reads, 3 with the TMA-staged
 // tile; else, and when a form does not apply, the plain per-element form.
 template <class S>
 inline int launch_sweep_col(doe_ctx* c, const ColSweepBase& op, int nplanes, int ncols, int form) {
+  if constexpr (S::N >= 16 && S::N <= 4096 && sweep_res_smem<S>() <= 200 * 1024) {
+    if (c->tune_sweep_res > 1) {
+      const int rc = launch_sweep_res<S>(c, op, nplanes, ncols, c->tune_sweep_res);
+      if (rc != DOE_ERR_UNSUPPORTED) return rc;
+    }
+  }
   if constexpr (S::N >= 16 && S::N <= 4096 && sweep_tma_smem<S>() <= 200 * 1024) {
     if (form == 3) {
       const int rc = launch_sweep_tma<S>(c, op, nplanes, ncols);

@@ -76,7 +76,9 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * disable CUDA-graph replay of repeated device sweeps; "sweep_hsym" = 1 to have
  * the sweep column pass evaluate the transfer function once per pair of mirrored
  * rows (H depends on fy^2) into shared memory, 2 to also have its spectrum tile
- * staged into shared memory by TMA; "sweep_tc" = 0 to run
+ * staged into shared memory by TMA; "sweep_res" = K in 2..64 to have one CTA of
+ * the sweep column pass keep its spectrum tile in shared memory (one TMA copy)
+ * across K planes (1, the default: one plane per CTA); "sweep_tc" = 0 to run
  * 1024 x 1024 focus sweeps on the FP32 CUDA-core passes instead of the tcgen05
  * tensor-core passes (default 1); "design_cluster" = 1 to run image-plane
  * weightedGerchbergSaxton on square 64^2, 128^2 and 256^2 grids as one
@@ -93,12 +95,12 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
 /* Current value of "sweep_group", "sweep_fused", "sweep_graph", "sweep_hsym",
- * "sweep_tc", "design_cluster" or "surrogate_tc". */
+ * "sweep_res", "sweep_tc", "design_cluster" or "surrogate_tc". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for
- * the plain FFT and focus-sweep passes (and the sweep column pass's three load
- * formulations: "sweep_fused", "sweep_hsym"), then times the pipelined sweep for
+ * the plain FFT and focus-sweep passes (and the sweep column pass's load
+ * formulations: "sweep_fused", "sweep_hsym", "sweep_res" 2/4/8), then times the pipelined sweep for
  * several group sizes ("sweep_group") on the CUDA-core passes and, for 1024^2
  * grids with "sweep_tc" on, on the tensor-core passes, keeping the fastest pair
  * ("sweep_tc", "sweep_group"). chosen (5 ints, may be NULL) receives the picked

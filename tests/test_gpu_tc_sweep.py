@@ -155,3 +155,30 @@ def test_mirrored_row_transfer_function_form(engine, oracle):
     assert np.array_equal(outs[2], outs[0])  # ... and the spectrum staged by TMA
     for k in (0, 2):
         assert rel_l2(outs[2][k].ravel(), oracle_plane(oracle, f[0], 532e-9, zs[k])) < 1e-5
+
+
+def test_spectrum_resident_multi_plane_form(engine, oracle):
+    """The sweep column pass that keeps a CTA's spectrum tile in shared memory across
+    K planes ("sweep_res" K; one TMA copy per tile) gives the one-plane-per-CTA pass's
+    planes bitwise, including a last group shorter than K, and the oracle's."""
+    f = smooth_field(N, DX, 43)[None]
+    zs = np.array([0.013, 0.021, 0.034, 0.047, 0.058])
+    outs = {}
+    for res in (1, 2, 4, 8):
+        ctx = make_ctx(engine, 0, graph=0)
+        ctx.check(ctx.lib.doe_ctx_set_tuning(ctx.h, b"sweep_fused", 1))
+        ctx.check(ctx.lib.doe_ctx_set_tuning(ctx.h, b"sweep_res", res))
+        v = C.c_longlong(0)
+        ctx.check(ctx.lib.doe_ctx_get_tuning(ctx.h, b"sweep_res", C.byref(v)))
+        assert v.value == res
+        outs[res] = sweep(ctx, f, np.array([532e-9]), zs)
+        ctx.close()
+    for res in (2, 4, 8):
+        print(f"sweep_res {res} bitwise equal to one plane per CTA:", np.array_equal(outs[res], outs[1]))
+        assert np.array_equal(outs[res], outs[1])
+    for k in (0, 4):
+        assert rel_l2(outs[4][k].ravel(), oracle_plane(oracle, f[0], 532e-9, zs[k])) < 1e-5
+    ctx = make_ctx(engine, 0, graph=0)
+    assert ctx.lib.doe_ctx_set_tuning(ctx.h, b"sweep_res", 0) != 0
+    assert ctx.lib.doe_ctx_set_tuning(ctx.h, b"sweep_res", 65) != 0
+    ctx.close()
