@@ -16,7 +16,10 @@ int time_design(doe_ctx* c, const doe_design_dev_desc& d, const float* phase0, s
   float best = 1e30f;
   cudaEvent_t a, b;
   DOE_CUDA(c, cudaEventCreate(&a));
-  DOE_CUDA(c, cudaEventCreate(&b));
+  if (cudaEventCreate(&b) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return set_err(c, DOE_ERR_CUDA, "autotune design: event creation failed");
+  }
   int rc = DOE_OK;
   for (int r = 0; r < 3 && rc == DOE_OK; ++r) {
     if (cudaMemcpyAsync(d.phase, phase0, phase_bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
@@ -52,9 +55,8 @@ extern "C" int doe_autotune_design(doe_ctx* c, const doe_design_dev_desc* desc, 
   const size_t pbytes = sizeof(float) * (size_t)d.batch * nx * ny;
   float* phase0 = nullptr;
   DOE_CUDA(c, cudaMalloc(&phase0, pbytes));
-  int rc = cudaMemcpyAsync(phase0, desc->phase, pbytes, cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess
-               ? DOE_OK
-               : set_err(c, DOE_ERR_CUDA, "autotune design: phase copy failed");
+  const bool saved = cudaMemcpyAsync(phase0, desc->phase, pbytes, cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess;
+  int rc = saved ? DOE_OK : set_err(c, DOE_ERR_CUDA, "autotune design: phase copy failed");
 
   const int lx = ilog2i(nx), ly = ilog2i(ny);
   const int nr = design_row_variants(nx), nc = design_col_variants(ny);
@@ -83,9 +85,10 @@ extern "C" int doe_autotune_design(doe_ctx* c, const doe_design_dev_desc* desc, 
     rc = time_design(c, d, phase0, pbytes, &best_cluster);
   }
   best_cl = best_cluster < best_pass ? 1 : 0;
-  // restore the caller's initial phase; keep the fastest configuration (or the
-  // previous one when a trial failed)
-  if (rc == DOE_OK && cudaMemcpyAsync(desc->phase, phase0, pbytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+  // restore the caller's initial phase, also after a failed trial; keep the
+  // fastest configuration (or the previous one when a trial failed)
+  if (saved && cudaMemcpyAsync(desc->phase, phase0, pbytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess &&
+      rc == DOE_OK)
     rc = set_err(c, DOE_ERR_CUDA, "autotune design: phase restore failed");
   cudaStreamSynchronize(c->stream);
   cudaFree(phase0);
