@@ -627,6 +627,159 @@ def profile_read(E, ctx):
     return out
 
 
+# ----------------------------------------------------------------- widened rows
+# The reference's other callers of the transforms (Fresnel propagation, focus stack
+# and full screen metrics, error-diffusion quantiser, hologram reconstruction):
+# each timed through its reference-facing C-ABI call with FP64 host planes (the
+# only form the reference has), with its device kernels timed alone by the
+# context's per-launch events and the FP64 C restatement timed on one host core.
+WR_LAM, WR_Z = 532e-9, 0.03
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _row_block(ctx, metric, unit, units, call, alg_bytes, basis, h2d, d2h, reps, cpu_fn, cpu_units, cpu_desc,
+               config):
+    """Time `call` (one reference-facing call, `units` units of work) end to end,
+    then once more with per-launch device timing; `alg_bytes` is the call's
+    algorithmic device traffic (the roofline basis)."""
+    L = ctx.lib
+    for _ in range(3):
+        call()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        call()
+    dt = (time.perf_counter() - t0) / reps
+    L.doe_ctx_set_profiling(ctx.h, 1)
+    call()
+    prof = profile_read(None, ctx)
+    L.doe_ctx_set_profiling(ctx.h, 0)
+    dev_ms = sum(v[0] for v in prof.values())
+    name, (kms, kcnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else None
+    out = {"metric": metric, "value": units / dt, "unit": unit, "ms_per_call": dt * 1e3, "config": config,
+           "e2e": {"value": units / dt, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "device": {"value": units / (dev_ms / 1e3) if dev_ms > 0 else None, "unit": unit,
+                      "kernel_ms_per_call": dev_ms,
+                      "note": "sum of the call's kernel durations (each launch timed alone), copies excluded"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak if achieved else None, "peak_kind": peak_kind, "basis": basis,
+                        "algorithmic_bytes_per_call": alg_bytes, "dominant_kernel": name,
+                        "dominant_share": kms / dev_ms if dev_ms > 0 else None, "traffic": None,
+                        "per_kernel_ms": {k: round(v[0], 4) for k, v in prof.items()}}}
+    if cpu_fn is not None:
+        t0 = time.perf_counter()
+        cpu_fn()
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cpu_units / tc, "unit": unit, "cores": 1, "kind": "port",
+                               "sample": cpu_desc}
+    return out
+
+
+def measure_widened(ctx, cpu):
+    """One block per widened row, each a few seconds of GPU and host time."""
+    O = None
+    if cpu:
+        from oracle import oracle as O
+        O.build()
+    L = ctx.lib
+    rng = np.random.default_rng(11)
+    out = {}
+
+    # f1: propagateFresnelFFT, 1024^2 beam with a seeded phase screen
+    n1 = 1024
+    y, x = np.mgrid[0:n1, 0:n1]
+    r2 = ((x - n1 / 2) ** 2 + (y - n1 / 2) ** 2) * DX * DX
+    amp = np.exp(-r2 / (600e-6) ** 2).ravel()
+    phs = rng.uniform(-np.pi, np.pi, n1 * n1)
+    re, im = amp * np.cos(phs), amp * np.sin(phs)
+    ore, oim, od = np.empty(n1 * n1), np.empty(n1 * n1), np.empty(2)
+    out["fresnel"] = _row_block(
+        ctx, "1024^2 single-FFT Fresnel propagations/s (propagateFresnelFFT, FP64 host planes)", "props/s", 1,
+        lambda: ctx.check(L.doe_fresnel(ctx.h, _dp(re), _dp(im), n1, n1, DX, DX, WR_LAM, WR_Z, _dp(ore), _dp(oim),
+                                        _dp(od))),
+        n1 * n1 * 32, "32 B/px: FP64 complex plane read once and written once", n1 * n1 * 16, n1 * n1 * 16, 20,
+        (lambda: O.fresnel(re, im, n1, n1, DX, DX, WR_LAM, WR_Z)) if O else None, 1,
+        "one 1024^2 Fresnel propagation, FP64 C restatement of propagateFresnelFFT on one thread",
+        {"grid": [n1, n1], "pitch_um": DX * 1e6, "lambda_nm": 532, "z_mm": WR_Z * 1e3})
+
+    # f2: focus stack (ProjectorSystem.simulate at 16 distances, one forward FFT shared)
+    n2, nz, dx2 = 512, 16, 8e-6
+    y, x = np.mgrid[0:n2, 0:n2]
+    half = 0.45 * n2
+    illum = (((np.abs(x - n2 / 2) <= half) & (np.abs(y - n2 / 2) <= half)).astype(np.float64)).ravel()
+    phase2 = rng.uniform(-np.pi, np.pi, n2 * n2)
+    zs2 = np.linspace(0.025, 0.035, nz)
+    s_re, s_im, s_d = np.empty(nz * n2 * n2), np.empty(nz * n2 * n2), np.empty(2 * nz)
+    el_re, el_im = illum * np.cos(phase2), illum * np.sin(phase2)
+    out["focus_stack"] = _row_block(
+        ctx, "512^2 focus-stack planes/s (ProjectorSystem.simulate at 16 distances, FP64 host planes)",
+        "planes/s", nz,
+        lambda: ctx.check(L.doe_simulate_sweep(ctx.h, _dp(illum), _dp(phase2), n2, n2, dx2, dx2, WR_LAM, _dp(zs2),
+                                               nz, 1, 0, 1, _dp(s_re), _dp(s_im), _dp(s_d))),
+        n2 * n2 * (16 + nz * 24),
+        "16 B/px element in, then per plane 8 B/px shared spectrum read + 16 B/px FP64 plane written",
+        n2 * n2 * 16, nz * n2 * n2 * 16, 10,
+        (lambda: [O.asm(el_re, el_im, n2, n2, dx2, dx2, WR_LAM, z) for z in zs2[:2]]) if O else None, 2,
+        "2 band-limited 512^2 angular-spectrum planes of the element, FP64 C restatement on one thread",
+        {"grid": [n2, n2], "distances": nz, "z_mm": [25, 35], "band_limit": True})
+
+    # f2: screenMetrics, every field, on a 1024^2 screen
+    tgt = np.zeros((n1, n1))
+    tgt[384:640, 320:704] = 1.0
+    tgt = tgt.ravel()
+    roi = (tgt > 0).astype(np.float64)
+    ill1 = np.ones(n1 * n1)
+    ph1 = rng.uniform(-np.pi, np.pi, n1 * n1)
+    mout = np.empty(18)
+    out["screen_metrics"] = _row_block(
+        ctx, "1024^2 screenMetrics evaluations/s (every field, FP64 host planes)", "screens/s", 1,
+        lambda: ctx.check(L.doe_screen_metrics_full(ctx.h, _dp(re), _dp(im), n1, n1, DX, DX, _dp(tgt), _dp(roi),
+                                                    _dp(ill1), _dp(ph1), DX, DX, 0, 0, _dp(mout))),
+        n1 * n1 * 48, "48 B/px: six FP64 planes read once (field re/im, target, ROI, illumination, phase)",
+        n1 * n1 * 48, 18 * 8, 20,
+        (lambda: [O.screen_metrics_full(re, im, n1, n1, DX, DX, tgt, roi, ill1, ph1, DX, DX) for _ in range(10)])
+        if O else None, 10, "ten 1024^2 screenMetrics, FP64 C restatement on one thread",
+        {"grid": [n1, n1], "target": "binary rectangle with its ROI", "spot_grid": None})
+
+    # f3: errorDiffusionQuantize of 512 designs of 256^2 (the image-plane batch)
+    nb, n3 = 512, 256
+    ph3 = rng.uniform(-4.0, 4.0, nb * n3 * n3)
+    q3 = np.empty_like(ph3)
+    out["error_diffusion"] = _row_block(
+        ctx, "256^2 errorDiffusionQuantize phase maps/s (512 maps per call, 4 levels, serpentine)", "maps/s", nb,
+        lambda: ctx.check(L.doe_error_diffusion(ctx.h, nb, n3 * n3, 4, 1, 1, _dp(ph3), _dp(q3))),
+        nb * n3 * n3 * 16, "16 B/px: FP64 phase read once, FP64 levels written once (the scan is serial per map)",
+        nb * n3 * n3 * 8, nb * n3 * n3 * 8, 5,
+        (lambda: [O.error_diffusion(ph3[k * n3 * n3:(k + 1) * n3 * n3], 4) for k in range(64)]) if O else None, 64,
+        "64 maps of 256^2, FP64 C restatement of errorDiffusionQuantize on one thread",
+        {"maps": nb, "grid": [n3, n3], "levels": 4, "snake": True, "wrap_first": True})
+
+    # f4: reconstructHologram, 1024^2 plate lit by a tilted plane wave, +-z in one batch
+    kx = 2 * np.pi * 0.02 / DX
+    xs = (np.arange(n1 * n1) % n1) * DX
+    ref_re, ref_im = np.cos(kx * xs), np.sin(kx * xs)
+    pl_re = (np.abs(re + ref_re) ** 2 + im ** 2)
+    pl_re /= pl_re.max()
+    pl_im = np.zeros_like(pl_re)
+    h = [np.empty(n1 * n1) for _ in range(4)]
+    out["hologram"] = _row_block(
+        ctx, "1024^2 hologram reconstructions/s (reconstructHologram: real and virtual image, FP64 host planes)",
+        "reconstructions/s", 1,
+        lambda: ctx.check(L.doe_hologram_reconstruct(ctx.h, _dp(pl_re), _dp(pl_im), _dp(ref_re), _dp(ref_im), n1,
+                                                     n1, DX, DX, WR_LAM, WR_Z, 0, 1, 0.02, *[_dp(a) for a in h],
+                                                     None, None)),
+        n1 * n1 * 64, "64 B/px: plate and reference FP64 complex planes read, two FP64 complex images written",
+        n1 * n1 * 32, n1 * n1 * 32, 20,
+        (lambda: O.reconstruct_hologram(pl_re, pl_im, ref_re, ref_im, n1, n1, DX, DX, WR_LAM, WR_Z)) if O else None,
+        1, "one 1024^2 reconstruction (two angular-spectrum planes), FP64 C restatement on one thread",
+        {"grid": [n1, n1], "band_limit": False, "z_mm": WR_Z * 1e3})
+    return out
+
+
 # ----------------------------------------------------------------- CPU (oracle port)
 def cpu_sample(params, fields_np, nplanes, threads):
     """Time `nplanes` FP64 propagations of the workload on `threads` host threads."""
@@ -913,7 +1066,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-fields", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "wgs256", "multiplane2048", "farfield_uneven"])
+    ap.add_argument("--workload", default="sweep",
+                    choices=["sweep", "wgs256", "multiplane2048", "farfield_uneven", "widened_rows"])
     ap.add_argument("--designs", type=int, default=1024, help="designs per step of the WGS workload")
     ap.add_argument("--no-wgs", action="store_true", help="skip the WGS block of the default line")
     ap.add_argument("--no-extras", action="store_true",
@@ -958,6 +1112,12 @@ def main():
         return main_multiplane(args, ctx, device, rank, world, local)
     if args.workload == "farfield_uneven":
         return main_uneven(args, ctx, device, rank, world, local)
+    if args.workload == "widened_rows":
+        if rank == 0:
+            print(json.dumps({"workload": "widened_rows", **measure_widened(ctx, not args.no_cpu_baseline)}),
+                  flush=True)
+        ctx.close()
+        return 0
 
     params = workload_params(seed=2024 + rank)[:max(1, min(args.fields, NFIELDS))]
     nfields = len(params)
@@ -1132,6 +1292,8 @@ def main():
         extras["farfield_uneven"] = measure_uneven(ctx, device, 1, 2, cpu_on)
         torch.cuda.empty_cache()
         extras["multiplane2048"] = measure_multiplane(ctx, device, 1, 2, cpu_on, False)
+        torch.cuda.empty_cache()
+        extras["widened_rows"] = measure_widened(ctx, cpu_on)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,

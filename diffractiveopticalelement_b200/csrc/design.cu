@@ -15,6 +15,7 @@
 // the previous iteration's final pass already produced (src/doe.js:350-352 and
 // :417-419 take identical inputs); here it is computed once and reused.
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "design_ops.cuh"
@@ -333,21 +334,11 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   const bool fourier = d0.algorithm == DOE_ALG_FOURIER || d0.algorithm == DOE_ALG_WGS_FOURIER;
   const bool wgs = d0.algorithm == DOE_ALG_WGS || d0.algorithm == DOE_ALG_WGS_FOURIER;
   const int nf = has_roi ? 4 : 3;
-  // host staging of the FP64 inputs (converted to FP32 on the device)
-  std::vector<double> h((size_t)Bn * nf);
-  double* hill = h.data();
-  double* htgt = hill + Bn;
-  double* hph = htgt + Bn;
-  double* hroi = has_roi ? hph + Bn : nullptr;
   std::vector<double> lam(nb), zz(nb);
   bool same = true;
+  int ngen = 0;  // designs whose initial phase is the seeded random phase
   for (int i = 0; i < nb; ++i) {
-    memcpy(hill + i * n, d[i].illumination, n * sizeof(double));
-    memcpy(htgt + i * n, d[i].target_amp, n * sizeof(double));
-    if (has_roi) memcpy(hroi + i * n, d[i].roi, n * sizeof(double));
-    if (d[i].init_phase) memcpy(hph + i * n, d[i].init_phase, n * sizeof(double));
-    else if (fourier) random_phase_host(nx, ny, d[i].seed, hph + i * n);  // src/doe.js:651
-    else memset(hph + i * n, 0, n * sizeof(double));                       // flatPhase, src/doe.js:339
+    if (!d[i].init_phase && fourier) ++ngen;
     lam[i] = d[i].lambda;
     zz[i] = d[i].z;
     same = same && lam[i] == lam[0] && zz[i] == zz[0];
@@ -358,7 +349,29 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   DOE_TRY(ensure_slot(c, kSlotOut, fbytes + sizeof(double) * ((size_t)nb * Ih * 2 + nb) + 256, &pout));
   DOE_TRY(ensure_slot(c, kSlotParams, (size_t)Bn * sizeof(float) + 256, &pw));
   double* din = (double*)pin;
-  DOE_CUDA(c, cudaMemcpyAsync(din, h.data(), (size_t)Bn * nf * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // the FP64 inputs (converted to FP32 on the device) go straight from the caller's
+  // arrays; only seeded initial phases are made on the host first
+  std::unique_ptr<double[]> gen(ngen ? new double[(size_t)ngen * n] : nullptr);
+  {
+    double* dph = din + 2 * Bn;
+    auto up = [&](double* dst, const double* src) {
+      return cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    };
+    for (int i = 0, g = 0; i < nb; ++i) {
+      DOE_CUDA(c, up(din + i * n, d[i].illumination));
+      DOE_CUDA(c, up(din + Bn + i * n, d[i].target_amp));
+      if (has_roi) DOE_CUDA(c, up(din + 3 * Bn + i * n, d[i].roi));
+      if (d[i].init_phase) {
+        DOE_CUDA(c, up(dph + i * n, d[i].init_phase));
+      } else if (fourier) {
+        double* gp = gen.get() + (size_t)g++ * n;
+        random_phase_host(nx, ny, d[i].seed, gp);  // src/doe.js:651
+        DOE_CUDA(c, up(dph + i * n, gp));
+      } else {
+        DOE_CUDA(c, cudaMemsetAsync(dph + i * n, 0, n * sizeof(double), c->stream));  // flatPhase, src/doe.js:339
+      }
+    }
+  }
   float* f = (float*)pout;
   float* fill = f;
   float* ftgt = f + Bn;
@@ -402,23 +415,35 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   DOE_TRY(convert_back_launch(c, fph, o, Bn));
   DOE_TRY(convert_back_launch(c, famp, o + Bn, Bn));
   if (wgs) DOE_TRY(convert_back_launch(c, fw, o + 2 * Bn, Bn));
-  std::vector<double> hout((size_t)Bn * (wgs ? 3 : 2));
   std::vector<double> hh((size_t)nb * Ih * 2 + nb);
-  DOE_CUDA(c, cudaMemcpyAsync(hout.data(), o, hout.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   DOE_CUDA(c, cudaMemcpyAsync(hh.data(), hist, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   DOE_TRY(design_error_check(c));
+  // every result plane straight into the caller's array
+  std::unique_ptr<double[]> tmp;
+  auto down = [&](double* dst, const double* src) {
+    return cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  };
   for (int i = 0; i < nb; ++i) {
-    memcpy(r[i].phase, hout.data() + i * n, n * sizeof(double));
-    const double* am = hout.data() + Bn + i * n;
-    if (r[i].amplitude) memcpy(r[i].amplitude, am, n * sizeof(double));
-    if (r[i].intensity)
-      for (long k = 0; k < n; ++k) r[i].intensity[k] = am[k] * am[k];
-    if (wgs && r[i].weights) memcpy(r[i].weights, hout.data() + 2 * Bn + i * n, n * sizeof(double));
+    DOE_CUDA(c, down(r[i].phase, o + i * n));
+    if (r[i].amplitude || r[i].intensity) {
+      double* am = r[i].amplitude;
+      if (!am) {
+        if (!tmp) tmp.reset(new double[n]);
+        am = tmp.get();
+      }
+      DOE_CUDA(c, down(am, o + Bn + i * n));
+      if (r[i].intensity) {
+        DOE_CUDA(c, cudaStreamSynchronize(c->stream));
+        for (long k = 0; k < n; ++k) r[i].intensity[k] = am[k] * am[k];
+      }
+    }
+    if (wgs && r[i].weights) DOE_CUDA(c, down(r[i].weights, o + 2 * Bn + i * n));
     if (r[i].error) memcpy(r[i].error, hh.data() + (size_t)i * Ih, I * sizeof(double));
     if (r[i].efficiency) memcpy(r[i].efficiency, hh.data() + (size_t)nb * Ih + (size_t)i * Ih, I * sizeof(double));
     r[i].rmse = wgs ? hh[(size_t)nb * Ih * 2 + i] : 0.0;
   }
+  DOE_CUDA(c, cudaStreamSynchronize(c->stream));  // pinned result arrays complete asynchronously
   return DOE_OK;
 }
 
@@ -439,19 +464,24 @@ extern "C" int doe_multiplane(doe_ctx* c, int nx, int ny, double dx, double dy, 
   const long n = (long)nx * ny;
   const int Ih = std::max(I, 1);
   const int nf = 2 + P * (roi ? 2 : 1);
-  std::vector<double> h((size_t)n * nf);
-  memcpy(h.data(), illumination, n * sizeof(double));
-  if (init_phase) memcpy(h.data() + n, init_phase, n * sizeof(double));
-  else memset(h.data() + n, 0, n * sizeof(double));  // flatPhase (src/doe.js:568)
-  memcpy(h.data() + 2 * n, target_amp, (size_t)P * n * sizeof(double));
-  if (roi) memcpy(h.data() + (2 + P) * n, roi, (size_t)P * n * sizeof(double));
   void *pin, *pf, *p0;
   DOE_TRY(ensure_slot(c, kSlotIn, (size_t)n * nf * sizeof(double), &pin));
   DOE_TRY(ensure_slot(c, kSlotOut, (size_t)n * (nf + 1) * sizeof(float) + 256, &pf));
   DOE_TRY(ensure_slot(c, kSlotDesign0, (size_t)n * sizeof(float2) + (size_t)P * n * sizeof(float2) + 1024, &p0));
   double* din = (double*)pin;
   float* f = (float*)pf;
-  DOE_CUDA(c, cudaMemcpyAsync(din, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // the caller's planes straight to the device (no host-side gather)
+  DOE_CUDA(c, cudaMemcpyAsync(din, illumination, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (init_phase) {
+    DOE_CUDA(c, cudaMemcpyAsync(din + n, init_phase, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  } else {
+    DOE_CUDA(c, cudaMemsetAsync(din + n, 0, n * sizeof(double), c->stream));  // flatPhase (src/doe.js:568)
+  }
+  DOE_CUDA(c, cudaMemcpyAsync(din + 2 * n, target_amp, (size_t)P * n * sizeof(double), cudaMemcpyHostToDevice,
+                              c->stream));
+  if (roi)
+    DOE_CUDA(c, cudaMemcpyAsync(din + (2 + P) * n, roi, (size_t)P * n * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
   DOE_TRY(convert_launch(c, din, f, n * nf));
   char* q0 = (char*)p0;
   DesignBufs b;

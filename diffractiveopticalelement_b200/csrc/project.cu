@@ -233,17 +233,15 @@ extern "C" int doe_screen_metrics(doe_ctx* c, const double* re, const double* im
     return set_err(c, DOE_ERR_BAD_ARG, "screenMetrics: null plane");
   const long n = (long)nx * ny;
   const int nf = roi ? 5 : 4;
-  std::vector<double> h((size_t)n * nf);
-  memcpy(h.data(), re, n * sizeof(double));
-  memcpy(h.data() + n, im, n * sizeof(double));
-  memcpy(h.data() + 2 * n, target_irr, n * sizeof(double));
-  memcpy(h.data() + 3 * n, illumination, n * sizeof(double));
-  if (roi) memcpy(h.data() + 4 * n, roi, n * sizeof(double));
   void *pin, *pf;
-  DOE_TRY(ensure_slot(c, kSlotIn, h.size() * sizeof(double), &pin));
+  DOE_TRY(ensure_slot(c, kSlotIn, (size_t)n * nf * sizeof(double), &pin));
   DOE_TRY(ensure_slot(c, kSlotOut, (size_t)n * (nf + 1) * sizeof(float) + 64 * sizeof(double), &pf));
   double* din = (double*)pin;
-  DOE_CUDA(c, cudaMemcpyAsync(din, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // each plane straight from the caller's array (no host-side gather)
+  const double* planes[5] = {re, im, target_irr, illumination, roi};
+  for (int k = 0; k < nf; ++k)
+    DOE_CUDA(c, cudaMemcpyAsync(din + (size_t)k * n, planes[k], n * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
   float* f = (float*)pf;
   // complex64 field (interleaved) from the FP64 planes, FP32 copies of the rest
   {

@@ -175,22 +175,17 @@ extern "C" int doe_screen_metrics_full(doe_ctx* c, const double* re, const doubl
     return set_err(c, DOE_ERR_BAD_ARG, "screenMetrics: bad spot grid %dx%d", grid_cols, grid_rows);
   const long n = (long)nx * ny;
   const int nf = roi ? 6 : 5;
-  std::vector<double> h((size_t)n * nf);
-  memcpy(h.data(), re, n * sizeof(double));
-  memcpy(h.data() + n, im, n * sizeof(double));
-  memcpy(h.data() + 2 * n, target_irr, n * sizeof(double));
-  memcpy(h.data() + 3 * n, illumination, n * sizeof(double));
-  memcpy(h.data() + 4 * n, phase, n * sizeof(double));
-  if (roi) memcpy(h.data() + 5 * n, roi, n * sizeof(double));
   const unsigned G = blocks_for(n);
   const int cells = grid_cols * grid_rows;
   const size_t red = sizeof(double) * ((size_t)G * kP1 + 16 * 3) + 64 + sizeof(unsigned long long) * kPX +
                      sizeof(double) * (cells + 1) + 1024;
   void *pin, *pr;
-  DOE_TRY(ensure_slot(c, kSlotIn, h.size() * sizeof(double), &pin));
+  DOE_TRY(ensure_slot(c, kSlotIn, (size_t)n * nf * sizeof(double), &pin));
   DOE_TRY(ensure_slot(c, kSlotRed, red, &pr));
   double* d = (double*)pin;
-  DOE_CUDA(c, cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // each plane straight from the caller's array (no host-side gather)
+  const double* planes[6] = {re, im, target_irr, illumination, phase, roi};
+  for (int k = 0; k < nf; ++k) DOE_TRY(upload_f64(c, d + (size_t)k * n, planes[k], (size_t)n));
   char* q = (char*)pr;
   FullArgs a;
   memset(&a, 0, sizeof(a));

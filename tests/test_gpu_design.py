@@ -384,7 +384,8 @@ def test_uneven_sizes_in_one_submission_and_graph_relaunch(engine, oracle):
     m.close()
 
 
-@pytest.mark.parametrize("n,levels,snake", [(64, 4, True), (128, 8, True), (32, 2, False), (1, 4, True)])
+@pytest.mark.parametrize("n,levels,snake", [(64, 4, True), (128, 8, True), (32, 2, False), (1, 4, True),
+                                            (2, 4, True), (13, 3, True), (9, 5, False), (24, 4, True)])
 def test_error_diffusion_matches_oracle_bitwise(engine, oracle, n, levels, snake):
     """errorDiffusionQuantize (src/doe.js:185-226) on the GPU: bitwise the FP64 scan,
     for one plane and for a batch of planes in one call."""
@@ -398,6 +399,17 @@ def test_error_diffusion_matches_oracle_bitwise(engine, oracle, n, levels, snake
     from diffractiveopticalelement_b200 import DOEError
     with pytest.raises(DOEError, match="square grid"):
         engine.errorDiffusionQuantize(np.zeros(50), 4)
+
+
+def test_error_diffusion_batch_over_several_blocks(engine, oracle):
+    """70 planes in one call (three 32-thread blocks of scan chains, the last one
+    partly idle), rows whose length is not a multiple of the read-ahead chunk."""
+    rng = np.random.default_rng(70)
+    n = 37
+    phis = rng.uniform(-7, 7, (70, n * n))
+    got = engine.errorDiffusionQuantize(phis, 6)
+    for b in (0, 31, 32, 63, 64, 69):
+        assert np.array_equal(got[b], oracle.error_diffusion(phis[b], 6))
 
 
 def test_design_doe_levels_quantises_like_the_reference(engine, oracle):
