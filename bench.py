@@ -1113,6 +1113,9 @@ def main():
     if args.workload == "farfield_uneven":
         return main_uneven(args, ctx, device, rank, world, local)
     if args.workload == "widened_rows":
+        for item in (args.pin_tuning.split(",") if args.pin_tuning else []):
+            key, val = item.split("=")
+            ctx.check(L.doe_ctx_set_tuning(ctx.h, key.encode(), int(val)))
         if rank == 0:
             print(json.dumps({"workload": "widened_rows", **measure_widened(ctx, not args.no_cpu_baseline)}),
                   flush=True)

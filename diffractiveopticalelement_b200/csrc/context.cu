@@ -1,6 +1,8 @@
 // context.cu -- context lifetime, twiddle tables and host helpers of the C ABI.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "engine.cuh"
@@ -21,6 +23,8 @@ extern "C" int doe_ctx_create(int device, doe_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return DOE_ERR_CUDA;
   doe_ctx* c = new doe_ctx();
   c->device = device;
+  // three quarters of the host's threads (at most 12) stage pageable caller planes
+  c->host_copy_threads = (int)std::min<unsigned>(12u, std::max(1u, std::thread::hardware_concurrency() * 3 / 4));
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
@@ -65,6 +69,12 @@ extern "C" void doe_ctx_destroy(doe_ctx* c) {
     cudaStreamDestroy(c->aux);
   }
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->stream) cudaStreamSynchronize(c->stream);  // no DMA still reads a staging chunk
+  for (int b = 0; b < 2; ++b) {
+    if (c->stage[b]) cudaFreeHost(c->stage[b]);
+    if (c->stage_ev[b]) cudaEventDestroy(c->stage_ev[b]);
+  }
+  destroy_copy_pool(c->copy_pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -139,6 +149,8 @@ extern "C" int doe_ctx_get_tuning(doe_ctx* c, const char* key, long long* value)
     *value = c->tune_sweep_hsym;
   } else if (k == "sweep_res") {
     *value = c->tune_sweep_res;
+  } else if (k == "host_copy_threads") {
+    *value = c->host_copy_threads;
   } else if (k == "surrogate_tc") {
     *value = c->tune_surrogate_tc;
   } else if (k == "design_cluster") {
@@ -162,6 +174,13 @@ extern "C" int doe_ctx_set_tuning(doe_ctx* c, const char* key, long long value) 
   }
   if (k == "sweep_tc") {
     c->tune_sweep_tc = value ? 1 : 0;
+    return DOE_OK;
+  }
+  if (k == "host_copy_threads") {
+    if (value < 0 || value > 64) return set_err(c, DOE_ERR_BAD_ARG, "host_copy_threads must be in [0, 64]");
+    destroy_copy_pool(c->copy_pool);  // made again, with the new count, at the next staged copy
+    c->copy_pool = nullptr;
+    c->host_copy_threads = (int)value;
     return DOE_OK;
   }
   if (k == "sweep_res") {

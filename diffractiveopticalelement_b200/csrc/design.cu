@@ -354,19 +354,17 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   std::unique_ptr<double[]> gen(ngen ? new double[(size_t)ngen * n] : nullptr);
   {
     double* dph = din + 2 * Bn;
-    auto up = [&](double* dst, const double* src) {
-      return cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-    };
+    auto up = [&](double* dst, const double* src) { return host_upload(c, dst, src, n * sizeof(double)); };
     for (int i = 0, g = 0; i < nb; ++i) {
-      DOE_CUDA(c, up(din + i * n, d[i].illumination));
-      DOE_CUDA(c, up(din + Bn + i * n, d[i].target_amp));
-      if (has_roi) DOE_CUDA(c, up(din + 3 * Bn + i * n, d[i].roi));
+      DOE_TRY(up(din + i * n, d[i].illumination));
+      DOE_TRY(up(din + Bn + i * n, d[i].target_amp));
+      if (has_roi) DOE_TRY(up(din + 3 * Bn + i * n, d[i].roi));
       if (d[i].init_phase) {
-        DOE_CUDA(c, up(dph + i * n, d[i].init_phase));
+        DOE_TRY(up(dph + i * n, d[i].init_phase));
       } else if (fourier) {
         double* gp = gen.get() + (size_t)g++ * n;
         random_phase_host(nx, ny, d[i].seed, gp);  // src/doe.js:651
-        DOE_CUDA(c, up(dph + i * n, gp));
+        DOE_TRY(up(dph + i * n, gp));
       } else {
         DOE_CUDA(c, cudaMemsetAsync(dph + i * n, 0, n * sizeof(double), c->stream));  // flatPhase, src/doe.js:339
       }
@@ -416,29 +414,27 @@ extern "C" int doe_design_batch(doe_ctx* c, int nb, const doe_design_desc* d, do
   DOE_TRY(convert_back_launch(c, famp, o + Bn, Bn));
   if (wgs) DOE_TRY(convert_back_launch(c, fw, o + 2 * Bn, Bn));
   std::vector<double> hh((size_t)nb * Ih * 2 + nb);
-  DOE_CUDA(c, cudaMemcpyAsync(hh.data(), hist, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, hh.data(), hist, hh.size() * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   DOE_TRY(design_error_check(c));
   // every result plane straight into the caller's array
   std::unique_ptr<double[]> tmp;
-  auto down = [&](double* dst, const double* src) {
-    return cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  };
+  auto down = [&](double* dst, const double* src) { return host_download(c, dst, src, n * sizeof(double)); };
   for (int i = 0; i < nb; ++i) {
-    DOE_CUDA(c, down(r[i].phase, o + i * n));
+    DOE_TRY(down(r[i].phase, o + i * n));
     if (r[i].amplitude || r[i].intensity) {
       double* am = r[i].amplitude;
       if (!am) {
         if (!tmp) tmp.reset(new double[n]);
         am = tmp.get();
       }
-      DOE_CUDA(c, down(am, o + Bn + i * n));
+      DOE_TRY(down(am, o + Bn + i * n));
       if (r[i].intensity) {
         DOE_CUDA(c, cudaStreamSynchronize(c->stream));
         for (long k = 0; k < n; ++k) r[i].intensity[k] = am[k] * am[k];
       }
     }
-    if (wgs && r[i].weights) DOE_CUDA(c, down(r[i].weights, o + 2 * Bn + i * n));
+    if (wgs && r[i].weights) DOE_TRY(down(r[i].weights, o + 2 * Bn + i * n));
     if (r[i].error) memcpy(r[i].error, hh.data() + (size_t)i * Ih, I * sizeof(double));
     if (r[i].efficiency) memcpy(r[i].efficiency, hh.data() + (size_t)nb * Ih + (size_t)i * Ih, I * sizeof(double));
     r[i].rmse = wgs ? hh[(size_t)nb * Ih * 2 + i] : 0.0;
@@ -471,17 +467,15 @@ extern "C" int doe_multiplane(doe_ctx* c, int nx, int ny, double dx, double dy, 
   double* din = (double*)pin;
   float* f = (float*)pf;
   // the caller's planes straight to the device (no host-side gather)
-  DOE_CUDA(c, cudaMemcpyAsync(din, illumination, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, din, illumination, n * sizeof(double)));
   if (init_phase) {
-    DOE_CUDA(c, cudaMemcpyAsync(din + n, init_phase, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DOE_TRY(host_upload(c, din + n, init_phase, n * sizeof(double)));
   } else {
     DOE_CUDA(c, cudaMemsetAsync(din + n, 0, n * sizeof(double), c->stream));  // flatPhase (src/doe.js:568)
   }
-  DOE_CUDA(c, cudaMemcpyAsync(din + 2 * n, target_amp, (size_t)P * n * sizeof(double), cudaMemcpyHostToDevice,
-                              c->stream));
+  DOE_TRY(host_upload(c, din + 2 * n, target_amp, (size_t)P * n * sizeof(double)));
   if (roi)
-    DOE_CUDA(c, cudaMemcpyAsync(din + (2 + P) * n, roi, (size_t)P * n * sizeof(double), cudaMemcpyHostToDevice,
-                                c->stream));
+    DOE_TRY(host_upload(c, din + (2 + P) * n, roi, (size_t)P * n * sizeof(double)));
   DOE_TRY(convert_launch(c, din, f, n * nf));
   char* q0 = (char*)p0;
   DesignBufs b;
@@ -510,8 +504,8 @@ extern "C" int doe_multiplane(doe_ctx* c, int nx, int ny, double dx, double dy, 
   DOE_TRY(design_run_multiplane(c, b, 1, I, P, htab, f + 2 * n, roi ? f + (long)(2 + P) * n : nullptr));
   DOE_TRY(convert_back_launch(c, b.phase, din, n));
   std::vector<double> ppe((size_t)P * Ih);
-  DOE_CUDA(c, cudaMemcpyAsync(phase, din, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(ppe.data(), b.pp_err, ppe.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, phase, din, n * sizeof(double)));
+  DOE_TRY(host_download(c, ppe.data(), b.pp_err, ppe.size() * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   // per-iteration error: mean of the weighted per-plane errors (src/doe.js:601, :618-619)
   for (int it = 0; it < I; ++it) {
@@ -583,7 +577,7 @@ extern "C" int doe_multiplane_dev(doe_ctx* c, const doe_multiplane_dev_desc* a) 
   std::vector<double> lam(P, a->lambda), w(P, 1.0);
   if (a->weight)
     for (int p = 0; p < P; ++p) w[p] = a->weight[p];
-  DOE_CUDA(c, cudaMemcpyAsync(dw, w.data(), sizeof(double) * P, cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, dw, w.data(), sizeof(double) * P));
   DOE_TRY(build_htab(c, nx, ny, a->dx, a->dy, P, lam.data(), a->z, htab));
   DOE_TRY(design_run_multiplane(c, b, B, I, P, htab, a->target_amp, a->roi));
   if (I > 0 && (a->error || a->efficiency || a->per_plane_error)) {

@@ -45,6 +45,10 @@ struct doe_prof_rec {
   cudaEvent_t a, b;
 };
 
+namespace doe {
+struct CopyPool;
+}
+
 struct doe_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -76,6 +80,12 @@ struct doe_ctx {
   size_t slot_bytes[doe::kSlotCount] = {};
   void* pinned = nullptr;  // host staging for parameter uploads
   size_t pinned_bytes = 0;
+  // staging of pageable caller planes (host_copy.cu): two pinned chunks, the
+  // events of their last DMA, the host threads that fill and drain them
+  void* stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  doe::CopyPool* copy_pool = nullptr;
+  int host_copy_threads = 1;  // set from the host's threads at creation; 0: straight through the driver
 };
 
 namespace doe {
@@ -148,6 +158,13 @@ inline int ensure_slot(doe_ctx* c, int s, size_t bytes, void** out) {
   *out = c->slot[s];
   return DOE_OK;
 }
+
+// Host <-> device copies of caller planes: pageable planes of 1 MB or more are
+// staged through pinned chunks by host threads (host_copy.cu). Uploads are
+// stream-ordered; downloads have completed when the call returns.
+int host_upload(doe_ctx* c, void* d, const void* h, size_t bytes);
+int host_download(doe_ctx* c, void* h, const void* d, size_t bytes);
+void destroy_copy_pool(CopyPool* p);
 
 inline int ensure_pinned(doe_ctx* c, size_t bytes, void** out) {
   if (c->pinned_bytes < bytes) {

@@ -195,10 +195,10 @@ extern "C" int doe_hologram_record(doe_ctx* c, const double* obj_re, const doubl
   double *orr = d, *oi = d + n, *rr = d + 2 * n, *ri = d + 3 * n, *sre = d + 4 * n, *sim = d + 5 * n,
          *rec = d + 6 * n, *pre = d + 7 * n, *pim = d + 8 * n;
   unsigned long long* mx = (unsigned long long*)(d + 9 * n);
-  DOE_CUDA(c, cudaMemcpyAsync(orr, obj_re, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(oi, obj_im, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(rr, ref_re, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(ri, ref_im, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, orr, obj_re, n * sizeof(double)));
+  DOE_TRY(host_upload(c, oi, obj_im, n * sizeof(double)));
+  DOE_TRY(host_upload(c, rr, ref_re, n * sizeof(double)));
+  DOE_TRY(host_upload(c, ri, ref_im, n * sizeof(double)));
   DOE_CUDA(c, cudaMemsetAsync(mx, 0, sizeof(unsigned long long), c->stream));
   {
     LaunchScope ls(c, "hologram_record");
@@ -210,11 +210,11 @@ extern "C" int doe_hologram_record(doe_ctx* c, const double* obj_re, const doubl
     holo_encode_kernel<<<grid_n(n), 256, 0, c->stream>>>(sre, sim, rec, n, mx, encode, levels, pre, pim);
     DOE_CUDA(c, cudaGetLastError());
   }
-  DOE_CUDA(c, cudaMemcpyAsync(plate_re, pre, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(plate_im, pim, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(recorded, rec, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (sum_re) DOE_CUDA(c, cudaMemcpyAsync(sum_re, sre, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (sum_im) DOE_CUDA(c, cudaMemcpyAsync(sum_im, sim, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, plate_re, pre, n * sizeof(double)));
+  DOE_TRY(host_download(c, plate_im, pim, n * sizeof(double)));
+  DOE_TRY(host_download(c, recorded, rec, n * sizeof(double)));
+  if (sum_re) DOE_TRY(host_download(c, sum_re, sre, n * sizeof(double)));
+  if (sum_im) DOE_TRY(host_download(c, sum_im, sim, n * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }
@@ -235,25 +235,25 @@ extern "C" int doe_hologram_reconstruct(doe_ctx* c, const double* plate_re, cons
   DOE_TRY(ensure_slot(c, kSlotOut, (size_t)8 * n * sizeof(double), &p));
   double* d = (double*)p;
   double *pr = d, *pi = d + n, *rr = d + 2 * n, *ri = d + 3 * n, *ore = d + 4 * n, *oim = d + 6 * n;
-  DOE_CUDA(c, cudaMemcpyAsync(pr, plate_re, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(pi, plate_im, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(rr, ref_re, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(ri, ref_im, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, pr, plate_re, n * sizeof(double)));
+  DOE_TRY(host_upload(c, pi, plate_im, n * sizeof(double)));
+  DOE_TRY(host_upload(c, rr, ref_re, n * sizeof(double)));
+  DOE_TRY(host_upload(c, ri, ref_im, n * sizeof(double)));
   {
     LaunchScope ls(c, "hologram_illum");
     holo_illum_kernel<<<grid_n(n), 256, 0, c->stream>>>(pr, pi, rr, ri, n, 2, ore, oim);
     DOE_CUDA(c, cudaGetLastError());
   }
-  if (illum_re) DOE_CUDA(c, cudaMemcpyAsync(illum_re, ore, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (illum_im) DOE_CUDA(c, cudaMemcpyAsync(illum_im, oim, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (illum_re) DOE_TRY(host_download(c, illum_re, ore, n * sizeof(double)));
+  if (illum_im) DOE_TRY(host_download(c, illum_im, oim, n * sizeof(double)));
   if (z != 0.0) {  // src/propagate.js:113: z = 0 leaves the field unchanged
     const double zz[2] = {z, -z};
     DOE_TRY(asm_f64_planes(c, ore, oim, 2, nx, ny, dx, dy, lambda, zz, band_limit, evanescent, soft_edge));
   }
-  DOE_CUDA(c, cudaMemcpyAsync(real_re, ore, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(real_im, oim, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(virt_re, ore + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(virt_im, oim + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, real_re, ore, n * sizeof(double)));
+  DOE_TRY(host_download(c, real_im, oim, n * sizeof(double)));
+  DOE_TRY(host_download(c, virt_re, ore + n, n * sizeof(double)));
+  DOE_TRY(host_download(c, virt_im, oim + n, n * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }
@@ -273,12 +273,12 @@ extern "C" int doe_modal_intensity(doe_ctx* c, int M, const double* re, const do
   double* dim = dre + (long)M * n;
   double* dout = dim + (long)M * n;
   double* dw = dout + n;
-  DOE_CUDA(c, cudaMemcpyAsync(dre, re, (size_t)M * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(dim, im, (size_t)M * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, dre, re, (size_t)M * n * sizeof(double)));
+  DOE_TRY(host_upload(c, dim, im, (size_t)M * n * sizeof(double)));
   double wsum = 0.0;
   if (weights) {
     for (int m = 0; m < M; ++m) wsum += weights[m];
-    DOE_CUDA(c, cudaMemcpyAsync(dw, weights, (size_t)M * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DOE_TRY(host_upload(c, dw, weights, (size_t)M * sizeof(double)));
   } else {
     wsum = M;
   }
@@ -291,7 +291,7 @@ extern "C" int doe_modal_intensity(doe_ctx* c, int M, const double* re, const do
     modal_sum_kernel<<<grid_n(n), 256, 0, c->stream>>>(dre, dim, M, n, weights ? dw : nullptr, wsum, dout);
     DOE_CUDA(c, cudaGetLastError());
   }
-  DOE_CUDA(c, cudaMemcpyAsync(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, out, dout, n * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }
@@ -330,7 +330,7 @@ extern "C" int doe_partially_coherent_modes(doe_ctx* c, int nx, int ny, double d
   double* d_tmp = d_ph + total;
   double* d_re = d_tmp + total;
   double* d_im = d_re + total;
-  DOE_CUDA(c, cudaMemcpyAsync(d_ph, ph.data(), total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, d_ph, ph.data(), total * sizeof(double)));
   {
     LaunchScope ls(c, "coherence_box_rows");
     const int rows = modes * ny;
@@ -344,8 +344,8 @@ extern "C" int doe_partially_coherent_modes(doe_ctx* c, int nx, int ny, double d
                                                                         waist * waist, d_re, d_im);
     DOE_CUDA(c, cudaGetLastError());
   }
-  DOE_CUDA(c, cudaMemcpyAsync(re, d_re, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(im, d_im, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, re, d_re, total * sizeof(double)));
+  DOE_TRY(host_download(c, im, d_im, total * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }

@@ -159,8 +159,8 @@ extern "C" int doe_simulate(doe_ctx* c, const double* illumination, const double
   double* dP = dA + n;
   float2* w = (float2*)pw;
   float2* w2 = (float2*)pw2;
-  DOE_CUDA(c, cudaMemcpyAsync(dA, illumination, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(dP, phase, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, dA, illumination, n * sizeof(double)));
+  DOE_TRY(host_upload(c, dP, phase, n * sizeof(double)));
   {
     LaunchScope ls(c, "element_field");
     element_field_kernel<<<grid_n(N), 256, 0, c->stream>>>(dA, dP, nx, ny, pad, far_field ? 1 : 0, w);
@@ -187,7 +187,7 @@ extern "C" int doe_simulate(doe_ctx* c, const double* illumination, const double
     void* pt;
     DOE_TRY(ensure_slot(c, kSlotTab, (nx + ny) * sizeof(float), &pt));
     float* cxy = (float*)pt;
-    DOE_CUDA(c, cudaMemcpyAsync(cxy, hc.data(), (nx + ny) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    DOE_TRY(host_upload(c, cxy, hc.data(), (nx + ny) * sizeof(float)));
     // the element was written ifftshifted; forward rows, then columns with the
     // fftshift + chirp on store
     DOE_TRY(with_row0(nx, [&](auto S) {
@@ -218,8 +218,8 @@ extern "C" int doe_simulate(doe_ctx* c, const double* illumination, const double
       out_d[1] = dy;
     }
   }
-  DOE_CUDA(c, cudaMemcpyAsync(out_re, ore, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(out_im, oim, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, out_re, ore, n * sizeof(double)));
+  DOE_TRY(host_download(c, out_im, oim, n * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }
@@ -240,8 +240,7 @@ extern "C" int doe_screen_metrics(doe_ctx* c, const double* re, const double* im
   // each plane straight from the caller's array (no host-side gather)
   const double* planes[5] = {re, im, target_irr, illumination, roi};
   for (int k = 0; k < nf; ++k)
-    DOE_CUDA(c, cudaMemcpyAsync(din + (size_t)k * n, planes[k], n * sizeof(double), cudaMemcpyHostToDevice,
-                                c->stream));
+    DOE_TRY(host_upload(c, din + (size_t)k * n, planes[k], n * sizeof(double)));
   float* f = (float*)pf;
   // complex64 field (interleaved) from the FP64 planes, FP32 copies of the rest
   {
@@ -268,7 +267,7 @@ extern "C" int doe_screen_metrics(doe_ctx* c, const double* re, const double* im
   a.dy = dy;
   a.out = dout;
   DOE_TRY(screen_metrics_launch(c, 1, a, kSlotParams));
-  DOE_CUDA(c, cudaMemcpyAsync(out, dout, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, out, dout, 6 * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }

@@ -209,7 +209,7 @@ extern "C" int doe_screen_metrics_full(doe_ctx* c, const double* re, const doubl
   // group g of pass p uses totals[g * K]: pass 1 group 0 (K=kP1 <= 16), pass 2 group 1 (K=kP2), ssim group 2 (K=2)
   unsigned long long ext0[kPX] = {0ull, 0ull, 0ull, 0x7ff0000000000000ull, 0ull};
   DOE_CUDA(c, cudaMemsetAsync(a.counters, 0, sizeof(unsigned) * 16, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(a.ext, ext0, sizeof(ext0), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, a.ext, ext0, sizeof(ext0)));
   if (cells) DOE_CUDA(c, cudaMemsetAsync(a.cells, 0, sizeof(double) * cells, c->stream));
   {
     LaunchScope ls(c, "screen_metrics_pass1");
@@ -218,8 +218,8 @@ extern "C" int doe_screen_metrics_full(doe_ctx* c, const double* re, const doubl
   }
   double t1[kP1];
   unsigned long long e1[kPX];
-  DOE_CUDA(c, cudaMemcpyAsync(t1, a.totals, sizeof(t1), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(e1, a.ext, sizeof(e1), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, t1, a.totals, sizeof(t1)));
+  DOE_TRY(host_download(c, e1, a.ext, sizeof(e1)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   double maxRoi, maxAll, maxT;
   memcpy(&maxRoi, &e1[kMaxRoi], 8);
@@ -252,9 +252,9 @@ extern "C" int doe_screen_metrics_full(doe_ctx* c, const double* re, const doubl
   double tot[48];
   unsigned long long e2[kPX];
   std::vector<double> hc(cells);
-  DOE_CUDA(c, cudaMemcpyAsync(tot, a.totals, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(e2, a.ext, sizeof(e2), cudaMemcpyDeviceToHost, c->stream));
-  if (cells) DOE_CUDA(c, cudaMemcpyAsync(hc.data(), a.cells, sizeof(double) * cells, cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, tot, a.totals, sizeof(tot)));
+  DOE_TRY(host_download(c, e2, a.ext, sizeof(e2)));
+  if (cells) DOE_TRY(host_download(c, hc.data(), a.cells, sizeof(double) * cells));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   const double* t2 = tot + kP2;       // group 1 of K = kP2
   const double* t3 = tot + 2 * 2;     // group 2 of K = 2

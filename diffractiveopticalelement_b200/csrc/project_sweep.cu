@@ -98,8 +98,8 @@ extern "C" int doe_simulate_sweep(doe_ctx* c, const double* illumination, const 
   float2* spec = elem + N;     // its forward spectrum
   double* ore = (double*)pout;
   double* oim = ore + (long)nz * n;
-  DOE_CUDA(c, cudaMemcpyAsync(dA, illumination, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(dP, phase, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, dA, illumination, n * sizeof(double)));
+  DOE_TRY(host_upload(c, dP, phase, n * sizeof(double)));
   {
     LaunchScope ls(c, "element_field");
     element_field_kernel<<<grid_for_n(N), 256, 0, c->stream>>>(dA, dP, nx, ny, pad, far_field ? 1 : 0, elem);
@@ -134,7 +134,7 @@ extern "C" int doe_simulate_sweep(doe_ctx* c, const double* illumination, const 
     void* pt;
     DOE_TRY(ensure_slot(c, kSlotTab, h.size() * sizeof(float), &pt));
     float* dt = (float*)pt;
-    DOE_CUDA(c, cudaMemcpyAsync(dt, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    DOE_TRY(host_upload(c, dt, h.data(), h.size() * sizeof(float)));
     LaunchScope ls(c, "focal_planes");
     focal_planes_kernel<<<grid_for_n((long)nz * n), 256, 0, c->stream>>>(spec, nx, ny, nz, dt,
                                                                          dt + (size_t)nz * (nx + ny), ore, oim);
@@ -178,8 +178,8 @@ extern "C" int doe_simulate_sweep(doe_ctx* c, const double* illumination, const 
         out_d[2 * p + 1] = dy;
       }
   }
-  DOE_CUDA(c, cudaMemcpyAsync(out_re, ore, (size_t)nz * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  DOE_CUDA(c, cudaMemcpyAsync(out_im, oim, (size_t)nz * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, out_re, ore, (size_t)nz * n * sizeof(double)));
+  DOE_TRY(host_download(c, out_im, oim, (size_t)nz * n * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }

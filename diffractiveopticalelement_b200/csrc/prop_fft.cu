@@ -5,14 +5,8 @@
 namespace doe {
 
 // ------------------------------------------------------------------ helpers
-int upload_f64(doe_ctx* c, double* d, const double* h, size_t n) {
-  DOE_CUDA(c, cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  return DOE_OK;
-}
-int download_f64(doe_ctx* c, double* h, const double* d, size_t n) {
-  DOE_CUDA(c, cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  return DOE_OK;
-}
+int upload_f64(doe_ctx* c, double* d, const double* h, size_t n) { return host_upload(c, d, h, n * sizeof(double)); }
+int download_f64(doe_ctx* c, double* h, const double* d, size_t n) { return host_download(c, h, d, n * sizeof(double)); }
 
 AsmGroupArgs group_args(int nx, int ny, double dx, double dy, int band_limit, int evanescent,
                                double soft_edge) {

@@ -145,7 +145,7 @@ extern "C" int doe_error_diffusion(doe_ctx* c, int batch, long long n, int level
   DOE_TRY(ensure_slot(c, kSlotIn, 2 * total * sizeof(double), &p));
   double* buf = (double*)p;
   double* o = buf + total;
-  DOE_CUDA(c, cudaMemcpyAsync(buf, phase, total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  DOE_TRY(host_upload(c, buf, phase, total * sizeof(double)));
   if (wrap_first) {
     LaunchScope ls(c, "wrap_phase");
     wrap_kernel<<<(unsigned)std::min<size_t>((total + 255) / 256, 148 * 16), 256, 0, c->stream>>>(buf, (long)total);
@@ -163,7 +163,7 @@ extern "C" int doe_error_diffusion(doe_ctx* c, int batch, long long n, int level
     wrap_kernel<<<(unsigned)std::min<size_t>((total + 255) / 256, 148 * 16), 256, 0, c->stream>>>(o, (long)total);
     DOE_CUDA(c, cudaGetLastError());
   }
-  DOE_CUDA(c, cudaMemcpyAsync(out, o, total * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  DOE_TRY(host_download(c, out, o, total * sizeof(double)));
   DOE_CUDA(c, cudaStreamSynchronize(c->stream));
   return DOE_OK;
 }

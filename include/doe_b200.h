@@ -89,13 +89,16 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * "surrogate_tc" selects the surrogate's convolution kernel where the layer
  * allows tcgen05 (a multiple of 64 input channels): 0 mma.sync, 1 tcgen05 with
  * cp.async operand staging, 2 tcgen05 with TMA operand staging and a 4-stage ring
- * (default), 3 the same with 3 stages;
+ * (default), 3 the same with 3 stages; "host_copy_threads" = host threads that
+ * stage pageable caller planes of 1 MB or more through pinned chunks of the
+ * context (default three quarters of the host's threads, at most 12; 0 = hand
+ * them to the driver as they are);
  * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
 int doe_ctx_set_tuning(doe_ctx* ctx, const char* key, long long value);
 /* Current value of "sweep_group", "sweep_fused", "sweep_graph", "sweep_hsym",
- * "sweep_res", "sweep_tc", "design_cluster" or "surrogate_tc". */
+ * "sweep_res", "sweep_tc", "design_cluster", "surrogate_tc" or "host_copy_threads". */
 int doe_ctx_get_tuning(doe_ctx* ctx, const char* key, long long* value);
 /* Autotuner (engine-only): times the compiled FFT-pass shape variants for an
  * nx-by-ny grid at the given geometry on this device and keeps the fastest for
