@@ -23,8 +23,9 @@ extern "C" int doe_ctx_create(int device, doe_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return DOE_ERR_CUDA;
   doe_ctx* c = new doe_ctx();
   c->device = device;
-  // three quarters of the host's threads (at most 12) stage pageable caller planes
-  c->host_copy_threads = (int)std::min<unsigned>(12u, std::max(1u, std::thread::hardware_concurrency() * 3 / 4));
+  // a quarter of the host's threads, at most 4, stage pageable caller planes (on a
+  // 16-thread host 4 were fastest: more contend for the memory bus and the cores)
+  c->host_copy_threads = (int)std::min<unsigned>(4u, std::max(1u, std::thread::hardware_concurrency() / 4));
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;

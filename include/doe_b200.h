@@ -91,8 +91,8 @@ int doe_ctx_profile_read(doe_ctx* ctx, int max_entries, char* names, int name_le
  * cp.async operand staging, 2 tcgen05 with TMA operand staging and a 4-stage ring
  * (default), 3 the same with 3 stages; "host_copy_threads" = host threads that
  * stage pageable caller planes of 1 MB or more through pinned chunks of the
- * context (default three quarters of the host's threads, at most 12; 0 = hand
- * them to the driver as they are);
+ * context (default a quarter of the host's threads, at most 4; 0 = hand them
+ * to the driver as they are);
  * "fft_row", "fft_col",
  * "sweep_row", "sweep_col", "design_row", "design_col" = (log2(n) << 8) | shape
  * variant for that pass. */
