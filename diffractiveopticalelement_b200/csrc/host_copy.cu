@@ -37,15 +37,23 @@ struct CopyPool {
   size_t bytes = 0;
 
   explicit CopyPool(int workers) {
-    for (int i = 0; i < workers; ++i) th.emplace_back([this, i] { work(i + 1); });
+    try {
+      for (int i = 0; i < workers; ++i) th.emplace_back([this, i] { work(i + 1); });
+    } catch (...) {  // a thread could not be started: stop the ones that were
+      shutdown();
+      throw;
+    }
   }
-  ~CopyPool() {
+  ~CopyPool() { shutdown(); }
+  void shutdown() {
     {
       std::lock_guard<std::mutex> l(m);
       stop = true;
     }
     go.notify_all();
-    for (auto& t : th) t.join();
+    for (auto& t : th)
+      if (t.joinable()) t.join();
+    th.clear();
   }
   void slice(int i) const {
     const size_t parts = th.size() + 1;
@@ -100,20 +108,34 @@ bool is_pinned(const void* h) {
   return a.type == cudaMemoryTypeHost;
 }
 
-int ensure_stage(doe_ctx* c) {
+// The pinned chunks, their events and the host threads, made at the first staged
+// copy. When any of them cannot be had (pinned memory or threads exhausted), the
+// context stops staging and hands its planes to the driver from then on.
+bool ensure_stage(doe_ctx* c) {
   if (!c->stage[0]) {
     for (int b = 0; b < 2; ++b) {
-      DOE_CUDA(c, cudaMallocHost(&c->stage[b], kChunk));
-      DOE_CUDA(c, cudaEventCreateWithFlags(&c->stage_ev[b], cudaEventDisableTiming));
-      DOE_CUDA(c, cudaEventRecord(c->stage_ev[b], c->stream));
+      if (cudaMallocHost(&c->stage[b], kChunk) != cudaSuccess ||
+          cudaEventCreateWithFlags(&c->stage_ev[b], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventRecord(c->stage_ev[b], c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        c->host_copy_threads = 0;
+        return false;
+      }
     }
   }
-  if (!c->copy_pool) c->copy_pool = new CopyPool(c->host_copy_threads - 1);
-  return DOE_OK;
+  if (!c->copy_pool) {
+    try {
+      c->copy_pool = new CopyPool(c->host_copy_threads - 1);
+    } catch (...) {
+      c->host_copy_threads = 0;
+      return false;
+    }
+  }
+  return true;
 }
 
 bool staged(doe_ctx* c, const void* h, size_t bytes) {
-  return c->host_copy_threads > 0 && bytes >= kStageMin && !is_pinned(h);
+  return c->host_copy_threads > 0 && bytes >= kStageMin && !is_pinned(h) && ensure_stage(c);
 }
 
 }  // namespace
@@ -123,7 +145,6 @@ int host_upload(doe_ctx* c, void* d, const void* h, size_t bytes) {
     DOE_CUDA(c, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream));
     return DOE_OK;
   }
-  DOE_TRY(ensure_stage(c));
   for (size_t off = 0, k = 0; off < bytes; off += kChunk, ++k) {
     const int b = (int)(k & 1);  // chunk k's buffer was last read by the DMA of chunk k - 2
     const size_t len = std::min(kChunk, bytes - off);
@@ -140,7 +161,6 @@ int host_download(doe_ctx* c, void* h, const void* d, size_t bytes) {
     DOE_CUDA(c, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c->stream));
     return DOE_OK;
   }
-  DOE_TRY(ensure_stage(c));
   // chunk k's DMA is queued before chunk k - 1 is copied out on the host; chunk
   // k's buffer was last read by the host copy of chunk k - 2, which has returned
   const size_t nch = (bytes + kChunk - 1) / kChunk;
