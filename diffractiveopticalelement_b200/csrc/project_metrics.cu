@@ -38,11 +38,18 @@ struct FullArgs {
   double C1, C2;
 };
 
+// Maxima / minima of non-negative values: folded over the warp first, then one
+// integer atomic per warp on the FP64 bit pattern (one atomic per thread on a
+// single address serialises every thread of the grid at that address).
 __device__ __forceinline__ void amax(unsigned long long* a, double v) {
-  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 __device__ __forceinline__ void amin(unsigned long long* a, double v) {
-  atomicMin(a, (unsigned long long)__double_as_longlong(v));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(a, (unsigned long long)__double_as_longlong(v));
 }
 
 __global__ void metrics_pass1(FullArgs a) {
@@ -51,7 +58,11 @@ __global__ void metrics_pass1(FullArgs a) {
 #pragma unroll
   for (int k = 0; k < kP1; ++k) acc.v[k] = 0.0;
   double mroi = 0.0, mall = 0.0, mt = 0.0;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+  // pixel coordinates advance with the grid stride (no division per pixel)
+  const long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x, stride = (long)gridDim.x * blockDim.x;
+  const int sx = (int)(stride % a.nx), sy = (int)(stride / a.nx);
+  int xi = (int)(i0 % a.nx), yi = (int)(i0 / a.nx);
+  for (long i = i0; i < n; i += stride) {
     const double irr = a.re[i] * a.re[i] + a.im[i] * a.im[i];
     const double m = a.roi ? a.roi[i] : 1.0;
     const double T = a.tgt[i];
@@ -76,10 +87,15 @@ __global__ void metrics_pass1(FullArgs a) {
     acc.v[kZr] += zr;
     acc.v[kZi] += zi;
     acc.v[kZp] += zr * zr + zi * zi;
-    const int xi = (int)(i % a.nx), yi = (int)(i / a.nx);
     const double x = (xi - a.nx / 2.0) * a.sdx, y = (yi - a.ny / 2.0) * a.sdy;
     acc.v[kRx] += irr * x * x;
     acc.v[kRy] += irr * y * y;
+    xi += sx;
+    yi += sy;
+    if (xi >= a.nx) {
+      xi -= a.nx;
+      ++yi;
+    }
   }
   amax(&a.ext[kMaxRoi], mroi);
   amax(&a.ext[kMaxAll], mall);
