@@ -401,6 +401,27 @@ def test_error_diffusion_matches_oracle_bitwise(engine, oracle, n, levels, snake
         engine.errorDiffusionQuantize(np.zeros(50), 4)
 
 
+@pytest.mark.parametrize("levels", [2, 3, 4, 8, 16])
+def test_error_diffusion_on_level_boundaries(engine, oracle, levels):
+    """Inputs on and next to the rounding boundaries of the quantiser (multiples of
+    half a level step, and their neighbouring doubles): bitwise the FP64 scan."""
+    step = 2 * np.pi / levels
+    k = np.arange(-2 * levels, 2 * levels + 1)
+    base = np.concatenate([(k + 0.5) * step, k * step, np.zeros(3)])
+    cand = np.concatenate([base, np.nextafter(base, np.inf), np.nextafter(base, -np.inf)])
+    rng = np.random.default_rng(levels)
+    n = 48
+    phis = rng.choice(cand, size=(4, n * n))
+    phis[3, ::7] = rng.uniform(-np.pi, np.pi, phis[3, ::7].shape)
+    for snake in (True, False):
+        got = engine.errorDiffusionQuantize(phis, levels, {"snake": snake})
+        for b in range(4):
+            assert np.array_equal(got[b], oracle.error_diffusion(phis[b], levels, snake=snake))
+        got = engine.errorDiffusionQuantize(phis, levels, {"snake": snake, "wrapFirst": False})
+        for b in range(4):
+            assert np.array_equal(got[b], oracle.error_diffusion(phis[b], levels, snake=snake, wrap_first=False))
+
+
 def test_error_diffusion_batch_over_several_blocks(engine, oracle):
     """70 planes in one call (three 32-thread blocks of scan chains, the last one
     partly idle), rows whose length is not a multiple of the read-ahead chunk."""
