@@ -706,6 +706,27 @@ def measure_widened(ctx, cpu):
         "one 1024^2 Fresnel propagation, FP64 C restatement of propagateFresnelFFT on one thread",
         {"grid": [n1, n1], "pitch_um": DX * 1e6, "lambda_nm": 532, "z_mm": WR_Z * 1e3})
 
+    # a5 / a2: the reference's basic calls on one 1024^2 plane, in place
+    w_re, w_im = re.copy(), im.copy()
+    out["asm"] = _row_block(
+        ctx, "1024^2 band-limited angular-spectrum propagations/s (propagateAngularSpectrumInPlace, FP64 host "
+             "planes)", "props/s", 1,
+        lambda: ctx.check(L.doe_asm(ctx.h, _dp(w_re), _dp(w_im), n1, n1, DX, DX, WR_LAM, WR_Z, 1, 1, 0.02)),
+        n1 * n1 * 32, "32 B/px: FP64 complex plane read once and written once", n1 * n1 * 16, n1 * n1 * 16, 20,
+        (lambda: O.asm(re, im, n1, n1, DX, DX, WR_LAM, WR_Z)) if O else None, 1,
+        "one 1024^2 band-limited propagation, FP64 C restatement of propagateAngularSpectrum on one thread",
+        {"grid": [n1, n1], "pitch_um": DX * 1e6, "lambda_nm": 532, "z_mm": WR_Z * 1e3, "band_limit": True})
+    def fft_pair():  # forward then inverse, so that the plane stays bounded over the repeats
+        ctx.check(L.doe_fft2d(ctx.h, _dp(w_re), _dp(w_im), n1, n1, 0))
+        ctx.check(L.doe_fft2d(ctx.h, _dp(w_re), _dp(w_im), n1, n1, 1))
+
+    out["fft2d"] = _row_block(
+        ctx, "1024^2 2-D FFTs/s (fft2d, FP64 host planes, in place; forward and inverse alternate)", "ffts/s", 2,
+        fft_pair, 2 * n1 * n1 * 32, "32 B/px per transform: FP64 complex plane read once and written once",
+        2 * n1 * n1 * 16, 2 * n1 * n1 * 16, 10,
+        (lambda: (O.fft2d(re, im, n1, n1), O.fft2d(re, im, n1, n1, inverse=True))) if O else None, 2,
+        "one forward and one inverse 1024^2 FFT, FP64 C restatement of fft2d on one thread", {"grid": [n1, n1]})
+
     # f2: focus stack (ProjectorSystem.simulate at 16 distances, one forward FFT shared)
     n2, nz, dx2 = 512, 16, 8e-6
     y, x = np.mgrid[0:n2, 0:n2]
