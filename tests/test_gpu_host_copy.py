@@ -69,3 +69,20 @@ def test_ragged_sizes_and_pinned_caller_buffers(engine, oracle):
     assert ctx.lib.doe_ctx_set_tuning(ctx.h, b"host_copy_threads", -1) != 0
     assert ctx.lib.doe_ctx_set_tuning(ctx.h, b"host_copy_threads", 65) != 0
     ctx.close()
+
+
+def test_design_host_call_through_staging(engine):
+    """designDOE on a 512^2 grid (2 MiB FP64 input and result planes, one staged copy
+    each): the same design with and without staging, bitwise."""
+    n = 512
+    yy, xx = np.mgrid[0:n, 0:n]
+    target = (((xx - n / 2) ** 2 + (yy - n / 2) ** 2) < (n / 6) ** 2).astype(np.float64).ravel()
+    cfg = {"nx": n, "ny": n, "dx": 8e-6, "lambda": 532e-9, "z": 0.03, "iterations": 3, "target": target,
+           "algorithm": "wgs"}
+    runs = {}
+    for threads in (0, 4):
+        ctx = _ctx(engine, threads)
+        r = engine.designDOE(dict(cfg), ctx=ctx)
+        runs[threads] = (np.array(r["phase"]), np.array(r["error"]))
+        ctx.close()
+    assert np.array_equal(runs[0][0], runs[4][0]) and np.array_equal(runs[0][1], runs[4][1])
