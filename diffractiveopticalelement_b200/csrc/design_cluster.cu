@@ -144,7 +144,7 @@ struct ClusterWgs {
                                            Store store, DAcc<K>& acc) const {
     constexpr int T = P::T, V = RS::V;
     const int lv = threadIdx.x / T, t = threadIdx.x % T;
-    SmemVec s{scratch + lv * padded_len<N>(), 1, 0};
+    SmemVec<> s{scratch + lv * padded_len<N>(), 1, 0};
 #pragma unroll 1
     for (int b0 = 0; b0 < G::ROWS; b0 += V) {
       const int yl = b0 + lv, y = row0 + yl;
@@ -170,7 +170,7 @@ struct ClusterWgs {
   __device__ __forceinline__ void col_asm(const Plane& pl, float2* scratch, int col0, const float2* htab) const {
     constexpr int C = CS::C;
     const int c = threadIdx.x % C, t = threadIdx.x / C;
-    SmemVec s{scratch, C, c};
+    SmemVec<P::PSHIFT> s{scratch, C, c};
 #pragma unroll 1
     for (int b0 = 0; b0 < G::ROWS; b0 += C) {
       const int x = col0 + b0 + c;

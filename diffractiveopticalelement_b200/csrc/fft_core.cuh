@@ -168,6 +168,16 @@ struct FftPlan {
   static constexpr __host__ __device__ int radix(int p) { return p == 0 ? R0 : (p == 1 ? R1 : R2); }
   static constexpr int last() { return radix(NP_ - 1); }
   static constexpr bool symmetric() { return R0 == radix(NP_ - 1); }
+  // Padding of the column kernels' exchanges (C vectors interleaved element by
+  // element): one spare slot every 2^PSHIFT complex values. The first pass stores
+  // with stride R0 per thread; a 64-bit access is served 16 lanes at a time by 16
+  // eight-byte banks, and one spare slot per 16 values keeps radix-8 and radix-16
+  // first passes conflict-free in that layout, where one per 32 left them 2-way
+  // conflicted on half of their stores; radix-32 first passes need one per 32.
+  // (Row kernels keep one per 32: with one per 16 the compiler's register
+  // allocation of the fused row operators grew, 64 -> 98 registers for the
+  // 256-point DOE update, and the occupancy lost outweighed the conflicts saved.)
+  static constexpr int PSHIFT = R0 >= 32 ? 5 : 4;
   static_assert(NP_ == 1 ? R0 == N_ : (NP_ == 2 ? R0 * R1 == N_ : R0 * R1 * R2 == N_), "radices must multiply to N");
 };
 
@@ -198,22 +208,33 @@ struct PassNs<P, 0> {
   static constexpr int value = 1;
 };
 
-// Padded shared-memory index: one spare slot every 32 complex values keeps the
-// stride-R Stockham writes of the early passes free of bank conflicts.
-__device__ __forceinline__ int spad(int x) { return x + (x >> 5); }
+// Padded shared-memory index: one spare slot every 2^SH complex values keeps the
+// stride-R Stockham writes of the early passes free of bank conflicts (SH = 5 for
+// row kernels, the plan's PSHIFT for column kernels).
+template <int SH>
+__device__ __forceinline__ int spad(int x) {
+  return x + (x >> SH);
+}
+// Shared-memory length (complex values) of one row kernel's padded vector.
 template <int N>
 constexpr int padded_len() {
   return N + N / 32 + 1;
+}
+// Shared-memory length of a column kernel's padded tile of len values.
+template <class P>
+constexpr int padded_col(int len) {
+  return len + (len >> P::PSHIFT) + 1;
 }
 
 // Vector accessor used for the shared-memory exchanges. Row kernels place each
 // vector contiguously (stride 1, vector pitch NPAD); column kernels interleave C
 // vectors (element-major, element stride C).
+template <int SH = 5>
 struct SmemVec {
   float2* base;
   int estride;  // distance between consecutive elements (1 or C)
   int off;      // vector offset inside an interleaved tile (column kernels)
-  __device__ __forceinline__ float2& at(int e) const { return base[spad(e * estride + off)]; }
+  __device__ __forceinline__ float2& at(int e) const { return base[spad<SH>(e * estride + off)]; }
 };
 
 // ---------------------------------------------------------------- one pass
@@ -242,8 +263,8 @@ __device__ __forceinline__ void pass_bfly(float2 (&v)[P::RMAX], int t, const flo
 }
 
 // Write pass-PI outputs to shared memory at their Stockham positions.
-template <class P, int PI>
-__device__ __forceinline__ void pass_store(const float2 (&v)[P::RMAX], int t, const SmemVec& s) {
+template <class P, int PI, class SV>
+__device__ __forceinline__ void pass_store(const float2 (&v)[P::RMAX], int t, const SV& s) {
   constexpr int R = P::radix(PI);
   constexpr int NS = PassNs<P, PI>::value;
 #pragma unroll
@@ -256,8 +277,8 @@ __device__ __forceinline__ void pass_store(const float2 (&v)[P::RMAX], int t, co
 }
 
 // Read pass-PI inputs from shared memory (element j + r N/R for butterfly j).
-template <class P, int PI>
-__device__ __forceinline__ void pass_load(float2 (&v)[P::RMAX], int t, const SmemVec& s) {
+template <class P, int PI, class SV>
+__device__ __forceinline__ void pass_load(float2 (&v)[P::RMAX], int t, const SV& s) {
   constexpr int R = P::radix(PI);
 #pragma unroll
   for (int b = 0; b < P::RMAX / R; ++b) {
@@ -284,9 +305,9 @@ __device__ __forceinline__ int out_elem(int t, int slot) {
 
 // Full transform: registers hold the pass-0 input layout on entry and the
 // natural-order output layout on return. `sync` is a block barrier.
-template <class P, bool INV, int PI = 0, class Sync>
-__device__ __forceinline__ void fft_run(float2 (&v)[P::RMAX], int t, const SmemVec& s,
-                                        const float2* __restrict__ tw, Sync sync) {
+template <class P, bool INV, int PI = 0, class SV, class Sync>
+__device__ __forceinline__ void fft_run(float2 (&v)[P::RMAX], int t, const SV& s, const float2* __restrict__ tw,
+                                        Sync sync) {
   pass_bfly<P, PI, INV, 0>(v, t, tw);
   if constexpr (PI + 1 < P::NP) {
     sync();  // everyone finished reading the previous contents of s
@@ -299,8 +320,8 @@ __device__ __forceinline__ void fft_run(float2 (&v)[P::RMAX], int t, const SmemV
 
 // Re-layout registers from the output layout to the pass-0 input layout (only
 // needed for asymmetric plans when two transforms are chained).
-template <class P, class Sync>
-__device__ __forceinline__ void relayout_out_to_in(float2 (&v)[P::RMAX], int t, const SmemVec& s, Sync sync) {
+template <class P, class SV, class Sync>
+__device__ __forceinline__ void relayout_out_to_in(float2 (&v)[P::RMAX], int t, const SV& s, Sync sync) {
   if constexpr (!P::symmetric()) {
     sync();
 #pragma unroll

@@ -27,7 +27,7 @@ struct NoAcc {};
 
 // CTA shapes. A row shape processes V vectors of a plane per CTA (one vector =
 // one row), a column shape C adjacent columns (element-major tile in shared
-// memory so a half-warp always touches one element row: conflict-free).
+// memory, the C columns of an element adjacent; padded per the plan's PSHIFT).
 template <class P, int V_, int MINB_ = 1>
 struct RowShape {
   using Plan = P;
@@ -47,7 +47,7 @@ struct ColShape {
   static constexpr int MINB = MINB_;  // CTAs per SM the register budget is sized for
   static constexpr int T = P::T;
   static constexpr int THREADS = C * T;
-  static constexpr int SMEM = P::NP > 1 ? (P::N * C + (P::N * C) / 32 + 1) * (int)sizeof(float2) : 0;
+  static constexpr int SMEM = P::NP > 1 ? padded_col<P>(P::N * C) * (int)sizeof(float2) : 0;
 };
 
 // Default shapes: ~256 threads per CTA (512 for the longest vectors).
@@ -214,7 +214,7 @@ __device__ __forceinline__ void row_pass(const Op& op, const float2* __restrict_
   const int line = bip * V + lv;
   const bool active = line < nlines;
   if (op_skip(op, plane)) return;
-  SmemVec s{smem + lv * padded_len<P::N>(), 1, 0};
+  SmemVec<> s{smem + lv * padded_len<P::N>(), 1, 0};
   auto st = op.init(plane, active ? line : 0);
   typename Op::Acc acc{};
   float2 v[RMAX];
@@ -261,7 +261,7 @@ __device__ __forceinline__ void col_pass(const Op& op, const float2* __restrict_
   const int line = blockIdx.x * C + c;
   const bool active = line < ncols;
   if (op_skip(op, plane)) return;
-  SmemVec s{smem, C, c};
+  SmemVec<P::PSHIFT> s{smem, C, c};
   auto st = op.init(plane, active ? line : 0);
   typename Op::Acc acc{};
   float2 v[RMAX];

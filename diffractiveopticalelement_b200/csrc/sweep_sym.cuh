@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(S::THREADS, S::MINB)
   const int plane = blockIdx.y;
   const int line = blockIdx.x * C + c;
   const bool active = line < ncols;
-  SmemVec s{smem, C, c};
+  SmemVec<P::PSHIFT> s{smem, C, c};
   const auto st = op.init(plane, active ? line : 0);
   float2 v[RMAX];
 #pragma unroll
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(S::THREADS, S::MINB)
     const int ky = in_elem<P>(t, q);
     v[q] = cmul(smem[ky * C + c], hs[(ky <= N / 2 ? ky : N - ky) * C + c]);
   }
-  SmemVec s{smem, C, c};  // the transform's exchanges reuse the tile's buffer (its first step is in registers)
+  SmemVec<P::PSHIFT> s{smem, C, c};  // the transform's exchanges reuse the tile's buffer (its first step is in registers)
   fft_run<P, true>(v, t, s, tw, BlockSync{});
   if (active) {
 #pragma unroll
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(S::THREADS, S::MINB)
     __syncthreads();
     return;
   }
-  SmemVec s{scratch, C, c};
+  SmemVec<P::PSHIFT> s{scratch, C, c};
   const int p0 = blockIdx.y * K;
 #pragma unroll 1
   for (int k = 0; k < K && p0 + k < nplanes; ++k) {
